@@ -1,0 +1,133 @@
+// zm_common.cuh -- shared device types and helpers of libzmodel_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "zm_plan.h"
+
+#define ZM_DEV __device__ __forceinline__
+
+namespace zm {
+
+// ------------------------------------------------------------------ complex
+template <typename R> struct cpx;
+template <> struct __align__(16) cpx<double> { double x, y; };
+template <> struct __align__(8) cpx<float> { float x, y; };
+
+template <typename R> ZM_DEV cpx<R> cadd(cpx<R> a, cpx<R> b) { return {a.x + b.x, a.y + b.y}; }
+template <typename R> ZM_DEV cpx<R> csub(cpx<R> a, cpx<R> b) { return {a.x - b.x, a.y - b.y}; }
+
+// Twiddle storage: FP64 pair for complex128, split hi/lo FP32 pairs for complex64
+// (w = hi + lo with hi = fl32(w), lo = fl32(w - hi), both from an FP64 value).
+template <typename R> struct tw;
+template <> struct __align__(16) tw<double> { double x, y; };
+template <> struct __align__(16) tw<float> { float x, y, lx, ly; };
+
+// a * w (forward sign) or a * conj(w) (CONJ).  complex64 applies the
+// compensated product a*hi + a*lo with every partial product fused.
+template <bool CONJ> ZM_DEV cpx<double> twmul(cpx<double> a, tw<double> w) {
+    const double wy = CONJ ? -w.y : w.y;
+    return {fma(a.x, w.x, -a.y * wy), fma(a.x, wy, a.y * w.x)};
+}
+template <bool CONJ> ZM_DEV cpx<float> twmul(cpx<float> a, tw<float> w) {
+    const float wy = CONJ ? -w.y : w.y;
+    const float ly = CONJ ? -w.ly : w.ly;
+    const float re_lo = fmaf(a.x, w.lx, -a.y * ly);
+    const float im_lo = fmaf(a.x, ly, a.y * w.lx);
+    return {fmaf(a.x, w.x, fmaf(-a.y, wy, re_lo)), fmaf(a.x, wy, fmaf(a.y, w.x, im_lo))};
+}
+template <typename R> ZM_DEV tw<R> ldtw(const tw<R> *t, int64_t i) { return __ldg(t + i); }
+template <> ZM_DEV tw<double> ldtw(const tw<double> *t, int64_t i) {
+    double2 v = __ldg(reinterpret_cast<const double2 *>(t) + i);
+    return {v.x, v.y};
+}
+template <> ZM_DEV tw<float> ldtw(const tw<float> *t, int64_t i) {
+    float4 v = __ldg(reinterpret_cast<const float4 *>(t) + i);
+    return {v.x, v.y, v.z, v.w};
+}
+
+template <typename R> ZM_DEV cpx<R> ldg(const cpx<R> *p) { return *p; }
+template <> ZM_DEV cpx<double> ldg(const cpx<double> *p) {
+    double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+    return {v.x, v.y};
+}
+template <> ZM_DEV cpx<float> ldg(const cpx<float> *p) {
+    float2 v = __ldg(reinterpret_cast<const float2 *>(p));
+    return {v.x, v.y};
+}
+
+// ----------------------------------------------------- radix-R DFT codelets
+// Constant twiddles w_R^k = exp(DIR * 2 pi i k / R), DIR = -1 forward, +1 inverse.
+// cos(2 pi k / 16) for k = 0..4 (cos pi/8, cos pi/4, cos 3pi/8).
+struct k16 {
+    static constexpr double c1 = 0.92387953251128675613;  // cos(pi/8)
+    static constexpr double c2 = 0.70710678118654752440;  // cos(pi/4)
+    static constexpr double c3 = 0.38268343236508977173;  // cos(3pi/8)
+};
+
+template <int R, int K, int DIR, typename T> ZM_DEV cpx<T> cmul_const(cpx<T> v) {
+    constexpr int k = ((K % R) + R) % R;
+    constexpr int k16i = k * (16 / R);        // position on the 16-point circle (R <= 16)
+    static_assert(16 % R == 0, "radix must divide 16");
+    if constexpr (k16i == 0) {
+        return v;
+    } else if constexpr (k16i == 8) {
+        return {-v.x, -v.y};
+    } else if constexpr (k16i == 4) {          // DIR=-1: -i, DIR=+1: +i
+        return DIR < 0 ? cpx<T>{v.y, -v.x} : cpx<T>{-v.y, v.x};
+    } else if constexpr (k16i == 12) {
+        return DIR < 0 ? cpx<T>{-v.y, v.x} : cpx<T>{v.y, -v.x};
+    } else {
+        // general: (c + DIR*i*s)
+        constexpr double cs[5] = {1.0, k16::c1, k16::c2, k16::c3, 0.0};
+        constexpr int q = k16i % 8;            // angle in (0, pi) modulo pi
+        constexpr double c0 = q <= 4 ? cs[q] : -cs[8 - q];
+        constexpr double s0 = q <= 4 ? cs[4 - q] : cs[q - 4];
+        constexpr double sgn = k16i >= 8 ? -1.0 : 1.0;   // add pi
+        constexpr double cc = sgn * c0, ss = sgn * s0 * (DIR < 0 ? -1.0 : 1.0);
+        const T c = (T)cc, s = (T)ss;
+        return {v.x * c - v.y * s, v.x * s + v.y * c};
+    }
+}
+
+template <int H, int R, int DIR, typename T, int K = 0> struct combine {
+    ZM_DEV static void run(cpx<T> *v, const cpx<T> *e, const cpx<T> *o) {
+        if constexpr (K < H) {
+            cpx<T> t = cmul_const<R, K, DIR>(o[K]);
+            v[K] = cadd(e[K], t);
+            v[K + H] = csub(e[K], t);
+            combine<H, R, DIR, T, K + 1>::run(v, e, o);
+        }
+    }
+};
+
+// In-register DFT of R points, natural order in and out (radix-2 DIT recursion
+// with the trivial rotations folded away).
+template <int R, int DIR, typename T> ZM_DEV void dft(cpx<T> *v) {
+    if constexpr (R == 1) {
+        return;
+    } else if constexpr (R == 2) {
+        cpx<T> a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else {
+        constexpr int H = R / 2;
+        cpx<T> e[H], o[H];
+#pragma unroll
+        for (int i = 0; i < H; i++) { e[i] = v[2 * i]; o[i] = v[2 * i + 1]; }
+        dft<H, DIR, T>(e);
+        dft<H, DIR, T>(o);
+        combine<H, R, DIR, T>::run(v, e, o);
+    }
+}
+
+// --------------------------------------------------------------- utilities
+ZM_DEV int64_t pack_pos(int64_t i, int logB, int64_t B, int logVEC) {   // block_cyclic_to_packed
+    return ((i & (B - 1)) << logVEC) + (i >> logB);
+}
+ZM_DEV int64_t unpack_pos(int64_t q, int64_t VEC, int logVEC, int logB) {  // inverse of pack_pos
+    return ((q & (VEC - 1)) << logB) + (q >> logVEC);
+}
+
+}  // namespace zm

@@ -1,0 +1,31 @@
+// zm_internal.h -- host-side declarations shared by the translation units of libzmodel_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "zm_plan.h"
+
+namespace zm {
+
+// launch bookkeeping
+void count_launch();
+int max_dyn_smem();
+
+// zm_fft.cu
+int ept_for(int dtype);
+cudaError_t launch_line_pass(const LineParams &prm, int dtype, bool inv, cudaStream_t st);
+
+// zm_stencil.cu
+enum StencilOp : int { ST_LAPLACE = 0, ST_DX = 1, ST_DY = 2 };
+cudaError_t launch_stencil(const zm_plan_s *p, int op, bool real_field, const void *in, void *out,
+                           double coef, cudaStream_t st);
+
+// zm_layout.cu
+cudaError_t launch_convert(const zm_plan_s *p, bool reciprocal, bool to_natural, const void *in,
+                           void *out, cudaStream_t st);
+cudaError_t launch_spectral(const zm_plan_s *p, void *data, int op, double a, cudaStream_t st);
+cudaError_t launch_fill(const zm_plan_s *p, void *data, int kind, uint64_t seed, cudaStream_t st);
+cudaError_t launch_fill_modes(const zm_plan_s *p, void *data, int nmodes, const int64_t *modes,
+                              const double *amps, double noise, uint64_t seed, cudaStream_t st);
+
+}  // namespace zm

@@ -1,0 +1,55 @@
+// zm_plan.h -- plan object and kernel parameter blocks of libzmodel_b200 (host + device).
+#pragma once
+
+#include <stddef.h>
+#include <stdint.h>
+
+namespace zm {
+
+// Which axis pass of a transform a line kernel runs.  Every pass reads each
+// global line (N points along one axis) from P contiguous rank chunks of L
+// points and writes it to the layout of the next stage of the reference
+// pipeline:
+//   X2  2D x pass: real layout -> layout after REPACK (fft.cu:207-269)
+//   Y2  2D y pass: layout after REPACK -> reciprocal layout (fft.cu:271-328)
+//   X3  3D x pass: real layout -> layout after REPACK_XY (fft3d.cu:246-298)
+//   Y3  3D y pass: after REPACK_XY -> after REPACK_YZ (fft3d.cu:300-352)
+//   Z3  3D z pass: after REPACK_YZ -> reciprocal layout (fft3d.cu:354-401)
+enum PassKind : int { PASS_X2 = 0, PASS_Y2 = 1, PASS_X3 = 2, PASS_Y3 = 3, PASS_Z3 = 4 };
+
+struct Geom {
+    int64_t n, b, p, L, vec, vp, m;
+    int logN, logB, logP, logL, logVEC, logVP, logM;
+    int dim;
+};
+
+// Parameters of one launch of the fused line kernel.
+struct LineParams {
+    Geom g;
+    int kind;          // PassKind
+    int T;             // lines per CTA (consecutive lines)
+    int64_t nlines;    // lines in this pass
+    const void *in;
+    void *out;
+    const void *twN;   // w_N^m, m < N, forward sign (tw<double> or tw<float>)
+    double scale_re, scale_im;
+    int apply_scale;   // multiply the stored values by scale
+    int permute_only;  // skip all arithmetic (reference do_compute=false)
+    // radix schedules of the two sub-transforms (first stage first)
+    int nst_vec, nst_m;
+    int rad_vec[8], rad_m[8];
+};
+
+}  // namespace zm
+
+struct zm_plan_s {
+    zm::Geom g;
+    int dtype;        // zm_dtype
+    unsigned flags;
+    int64_t ranks, rank_elems, total;
+    size_t elem_bytes;
+    int device;
+    void *twN;        // device twiddle table (N entries)
+    int T[3];         // lines per CTA for the passes (x, y, z)
+    int max_radix;
+};
