@@ -1,0 +1,387 @@
+"""Benchmark of the interleaved block-cyclic FFT + stencil hot path on B200.
+
+Workload (one step): the large 2D configuration -- N = 16384 (16384 x 16384), P = 4
+(16 virtual ranks), B = 64 -- on a field that is a seeded sum of 32 random Fourier
+modes (|k| <= N/8, unit complex Gaussian amplitudes) plus 1e-3 white noise:
+    forward FFT -> inverse FFT (round trip, scale 1/N^2) -> 5-point Laplacian,
+    4th-order dx and dy (h = 1/N) of the round-tripped field.
+The headline is the complex64 bulk form (compensated FP32 twiddles); the plain
+complex128 form is measured beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` is the device time of one step (ms, max over
+ranks, lower is better).  With --gpus N > 1 (torchrun) every rank runs an independent
+replica (the path is held on one GPU; there is no data-path collective).
+The reference arm (--impl reference) times the CPU restatement of the reference's
+pipeline (oracle/, FP64, all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N, P, B = 16384, 4, 64
+NMODES, NOISE, MODE_SEED, NOISE_SEED = 32, 1e-3, 1, 1
+METRIC = "fft_stencil_step_time"
+WORKLOAD = ("2D N=16384 P=4 B=64: forward FFT + inverse FFT + 5-pt Laplacian + dx + dy "
+            "(h=1/N) on 32 seeded Fourier modes + 1e-3 noise")
+# CPU sample: the same pipeline on an N=4096 grid (P=4, B=64), scaled to N=16384 by work
+CPU_SAMPLE_N = 4096
+
+
+def modes_and_amps(n: int):
+    """32 modes (kx, ky) uniform in the disc |k| <= n/8 (rejection sampling) and unit
+    complex Gaussian amplitudes, drawn from numpy.random.default_rng(seed=1)."""
+    import numpy as np
+    rng = np.random.default_rng(MODE_SEED)
+    kmax = n // 8
+    modes = []
+    while len(modes) < NMODES:
+        kx, ky = (int(v) for v in rng.integers(-kmax, kmax + 1, 2))
+        if kx * kx + ky * ky <= kmax * kmax:
+            modes.append((kx, ky))
+    amps = rng.standard_normal((NMODES, 2))
+    return np.array(modes, dtype=np.int64), amps
+
+
+def read_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def read_traffic(key: str):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary (profiles/traffic.txt)."""
+    p = ROOT / "profiles" / "traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == key:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                self.out = ""
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ CPU arm
+
+def cpu_sample(threads: int | None = None):
+    """Time the oracle (C restatement of the reference pipeline, FP64, OpenMP) on the
+    N=4096 sample and scale each part to N=16384 by its work."""
+    import numpy as np
+    import oracle as O
+    if threads:
+        O.set_threads(threads)
+    cores = O.max_threads()
+    n = CPU_SAMPLE_N
+    dim = 2
+    x = (O.uniform_field(0, n * n)).reshape(n, n)
+    buf = O.natural_to_real_layout(x, B, P)
+    t0 = time.perf_counter()
+    spec = O.forward_fft(buf, dim, n, B, P)
+    back = O.inverse_fft(spec, dim, n, B, P, scale=1.0 / n ** 2)
+    t1 = time.perf_counter()
+    O.laplace(back, dim, n, B, P)
+    O.dx(back, n, B, P, 1.0 / n)
+    O.dy(back, n, B, P, 1.0 / n)
+    t2 = time.perf_counter()
+    fft_scale = (N * N * math.log2(N * N)) / (n * n * math.log2(n * n))
+    st_scale = (N * N) / (n * n)
+    ms = ((t1 - t0) * fft_scale + (t2 - t1) * st_scale) * 1e3
+    sample = (f"oracle (C restatement of the reference pipeline, FP64, OpenMP) on N={n} P={P} B={B}: "
+              f"fwd+inv {1e3 * (t1 - t0):.1f} ms x{fft_scale:.2f} (N^2 log N), "
+              f"lap+dx+dy {1e3 * (t2 - t1):.1f} ms x{st_scale:.0f} (N^2)")
+    return ms, cores, sample
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        cpu_sample()
+    times = []
+    cores, sample = None, None
+    for _ in range(args.steps):
+        ms, cores, sample = cpu_sample()
+        times.append(ms)
+    v = statistics.mean(times)
+    line = {"metric": METRIC, "value": v, "unit": "ms", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": N, "p": P, "b": B},
+            "cpu_baseline": {"value": v, "unit": "ms", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+
+def run_ours(args, rank: int, world: int):
+    import numpy as np
+    import torch
+    from stencilfft_b200 import Plan, launch_count
+
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_
+        dist = dist_
+    stream = torch.cuda.current_stream()
+    modes, amps = modes_and_amps(N)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    def run_dtype(dt: str, timed_steps: int, warmup: int, with_e2e: bool):
+        pl = Plan(2, N, B, P, dtype=dt)
+        u = pl.empty()
+        pl.fill_modes(u, modes, amps, NOISE, NOISE_SEED)
+        spec, back, work = pl.empty(), pl.empty(), pl.empty()
+        lap, gx, gy = pl.empty(), pl.empty(), pl.empty()
+        h = 1.0 / N
+        marks = []
+
+        def step(record=None):
+            e = [ev() for _ in range(6)] if record is not None else None
+            if e: e[0].record(stream)
+            pl.forward_fft(u, spec, work=work)
+            if e: e[1].record(stream)
+            pl.inverse_fft(spec, back, scale=1.0 / (N * N), work=work)
+            if e: e[2].record(stream)
+            pl.laplace(back, lap, inv_h2=1.0 / (h * h))
+            if e: e[3].record(stream)
+            pl.dx(back, gx, delta=h)
+            if e: e[4].record(stream)
+            pl.dy(back, gy, delta=h)
+            if e: e[5].record(stream)
+            if record is not None:
+                record.append(e)
+
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        if dist: dist.barrier()
+        torch.cuda.synchronize()
+        l0 = launch_count()
+        t0, t1 = ev(), ev()
+        with ClockSampler(local) as cs:
+            t0.record(stream)
+            for _ in range(timed_steps):
+                step(marks)
+            t1.record(stream)
+            torch.cuda.synchronize()
+        launches = launch_count() - l0
+        if dist: dist.barrier()
+        ms = t0.elapsed_time(t1) / timed_steps
+        stage = {k: statistics.mean(m[i].elapsed_time(m[i + 1]) for m in marks)
+                 for i, k in enumerate(["fwd", "inv", "laplace", "dx", "dy"])}
+        # accuracy of the round trip, in FP64 on the device
+        err = float(torch.linalg.vector_norm((back - u).to(torch.complex128)) /
+                    torch.linalg.vector_norm(u.to(torch.complex128)))
+        res = {"ms": ms, "stage_ms": stage, "launches": launches, "clocks": cs.summary(),
+               "roundtrip_rel_l2": err, "field_bytes": pl.field_bytes}
+        if with_e2e:
+            # through the C ABI with host buffers: H2D input, the step, D2H of the outputs
+            host_in = torch.empty(pl.total, dtype=pl.torch_dtype, pin_memory=True)
+            host_in.copy_(u.cpu())
+            host_out = [torch.empty(pl.total, dtype=pl.torch_dtype, pin_memory=True) for _ in range(3)]
+            def e2e_step():
+                u.copy_(host_in, non_blocking=True)
+                step()
+                for hb, db in zip(host_out, (lap, gx, gy)):
+                    hb.copy_(db, non_blocking=True)
+            e2e_step()
+            torch.cuda.synchronize()
+            reps = max(1, min(timed_steps, 5))
+            a, b_ = ev(), ev()
+            a.record(stream)
+            for _ in range(reps):
+                e2e_step()
+            b_.record(stream)
+            torch.cuda.synchronize()
+            res["e2e_ms"] = a.elapsed_time(b_) / reps
+            res["h2d"] = pl.field_bytes
+            res["d2h"] = 3 * pl.field_bytes
+            del host_in, host_out
+        del u, spec, back, work, lap, gx, gy
+        pl.close()
+        torch.cuda.empty_cache()
+        return res
+
+    main = run_dtype("c64", args.steps, args.warmup, with_e2e=True)
+    side = None
+    try:
+        side = run_dtype("c128", max(2, args.steps // 2), max(3, args.warmup), with_e2e=False)
+    except Exception as ex:  # c128 at this N may be unsupported by the build
+        side = {"error": str(ex).splitlines()[0]}
+
+    def gmax(v: float) -> float:
+        if not dist:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ms = gmax(main["ms"])
+    e2e_ms = gmax(main["e2e_ms"])
+    F = main["field_bytes"]
+    peak, peak_kind = read_peaks()
+    # dominant kernel: the forward fused line pass (2 launches per forward call)
+    t_launch = main["stage_ms"]["fwd"] / 2
+    achieved = (2 * F) / (t_launch * 1e-3) / 1e9
+    traffic = read_traffic("line_fft_fwd_c64_N16384")
+    stages = {k: {"ms": round(v, 4), "GBps": round((4 * F if k in ("fwd", "inv") else 2 * F) / (v * 1e-3) / 1e9, 1)}
+              for k, v in main["stage_ms"].items()}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cms, cores, sample = cpu_sample()
+        cpu = {"value": round(cms, 2), "unit": "ms", "cores": cores, "kind": "port", "sample": sample}
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": round(ms, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64", "data": "synthetic (32 seeded Fourier modes + 1e-3 noise)",
+        "config": {"workload": WORKLOAD, "n": N, "p": P, "b": B, "dtype": "c64 (compensated FP32 twiddles)",
+                   "l2": "inputs larger than L2 (2 GiB field per buffer)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "kernel": "line_fft_kernel<float,16,fwd> (fused axis pass)",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": 2 * F},
+        "stages": stages,
+        "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": main["h2d"],
+                "d2h_bytes_per_step": main["d2h"]},
+        "gpu_launches": main["launches"],
+        "clocks": main["clocks"],
+        "accuracy": {"c64_roundtrip_rel_l2": main["roundtrip_rel_l2"]},
+        "c128": ({"ms": round(side["ms"], 4), "stage_ms": {k: round(v, 4) for k, v in side["stage_ms"].items()},
+                  "roundtrip_rel_l2": side["roundtrip_rel_l2"],
+                  "c128_over_c64": round(side["ms"] / main["ms"], 3)} if "ms" in side else side),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_profile_case(args):
+    """Small profiling case (N = 8192, c64 by default, 512 MiB per buffer): one warm-up
+    and one measured call of each stage, for `ncu -k ... -s/-c` captures."""
+    import torch
+    from stencilfft_b200 import Plan
+    n = args.profile_n
+    pl = Plan(2, n, B, P, dtype=args.profile_dtype)
+    modes, amps = modes_and_amps(n)
+    u = pl.empty()
+    pl.fill_modes(u, modes, amps, NOISE, NOISE_SEED)
+    spec, back, work, out = pl.empty(), pl.empty(), pl.empty(), pl.empty()
+    for _ in range(2):
+        pl.forward_fft(u, spec, work=work)
+        pl.inverse_fft(spec, back, scale=1.0 / (n * n), work=work)
+        pl.laplace(back, out, inv_h2=float(n * n))
+        pl.dx(back, out, delta=1.0 / n)
+        pl.dy(back, out, delta=1.0 / n)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_case": {"n": n, "p": P, "b": B, "dtype": args.profile_dtype,
+                                       "field_bytes": pl.field_bytes}}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="run the small profiling case only (for ncu captures)")
+    ap.add_argument("--profile-n", type=int, default=8192)
+    ap.add_argument("--profile-dtype", default="c64")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.profile_case:
+        run_profile_case(args)
+        return
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
