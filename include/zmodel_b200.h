@@ -115,6 +115,30 @@ int zm_fft_inverse(zm_plan plan, const void *in, void *out, void *work, double s
                    double scale_im, void *stream);
 
 /*
+ * zm_fft_inverse for callers that cannot allocate device memory (no counterpart in the
+ * reference).  zm_fft_inverse needs one field of intermediate storage: it overwrites
+ * `in`, or it uses a workspace the caller allocated.  Some callers can do neither -- a
+ * plugin whose host application owns every device allocation, or a loop under a fixed
+ * memory budget that may not grow or wait on an allocator -- and still need `in` kept.
+ * This call keeps `in` intact and takes the intermediate from a scratch array built
+ * into the library: a file-scope device array of ZM_STATIC_SCRATCH_BYTES (16 MiB) that
+ * every GPU which loads the library holds until the process exits.  It calls no
+ * allocator (no cudaMalloc / cudaFree, no allocating library routine).
+ *   - Limit: the field (zm_plan_info.field_bytes) must fit in 16 MiB, e.g. a 2D
+ *     complex128 field up to N = 1024 or a 3D complex64 field up to N = 128; larger
+ *     fields return ZM_ERR_WORKSPACE.
+ *   - The first call on each device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call before
+ *     any stream capture.
+ *   - All calls on a device share the one array, which keeps the previous call's
+ *     contents.  Each call overwrites everything it later reads, so nothing needs
+ *     clearing, but calls that overlap on the GPU (e.g. on two streams at once) race.
+ */
+#define ZM_STATIC_SCRATCH_BYTES (16u << 20)
+int zm_fft_inverse_static(zm_plan plan, const void *in, void *out, double scale_re,
+                          double scale_im, void *stream);
+
+/*
  * Stencils on the real-space layout.  Periodic boundaries over the whole N x N
  * (N^3) field; halos are read straight from the neighbouring virtual ranks.
  *

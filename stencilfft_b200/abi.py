@@ -58,6 +58,7 @@ SIGNATURES = {
     "zm_plan_workspace_size": [_P, ctypes.POINTER(ctypes.c_size_t)],
     "zm_fft_forward": [_P, _P, _P, _P, _P],
     "zm_fft_inverse": [_P, _P, _P, _P, _D, _D, _P],
+    "zm_fft_inverse_static": [_P, _P, _P, _D, _D, _P],
     "zm_laplace": [_P, _P, _P, _D, _P],
     "zm_dx": [_P, _P, _P, _D, _P],
     "zm_dy": [_P, _P, _P, _D, _P],

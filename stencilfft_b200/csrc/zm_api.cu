@@ -58,6 +58,16 @@ namespace zm {
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
+int report_error(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
 int max_dyn_smem() {
     static int cached[64];
     static std::once_flag once[64];

@@ -10,6 +10,8 @@ namespace zm {
 // launch bookkeeping
 void count_launch();
 int max_dyn_smem();
+// record `code` with a formatted message as the calling thread's last error; returns code
+int report_error(int code, const char *fmt, ...);
 
 // zm_fft.cu
 int ept_for(int dtype);
