@@ -128,6 +128,10 @@ static int pick_lines(const zm_plan_s *p) {
 }
 
 static bool fft_supported(const zm_plan_s *p, std::string *why) {
+    const bool permute = (p->flags & ZM_FLAG_PERMUTE_ONLY) != 0;
+    const int fused = p->dtype == ZM_C128 ? zm::fused_lines_c128(p->g.logVEC, p->g.logM)
+                                          : zm::fused_lines_c64(p->g.logVEC, p->g.logM);
+    if (fused > 0 && !permute) return true;
     const int ept = zm::ept_for(p->dtype);
     const int64_t threads = (int64_t)p->T[0] * p->g.n / ept;
     const int64_t smem = (int64_t)p->T[0] * p->g.n * (int64_t)p->elem_bytes;
@@ -147,6 +151,9 @@ static LineParams line_params(const zm_plan_s *p, int kind, const void *in, void
     lp.in = in;
     lp.out = out;
     lp.twN = p->twN;
+    lp.W = p->W;
+    lp.twv = p->twv;
+    lp.twm = p->twm;
     lp.scale_re = 1.0;
     lp.scale_im = 0.0;
     lp.apply_scale = 0;
@@ -264,38 +271,52 @@ int zm_plan_create(zm_plan *plan, int dim, int64_t n, int64_t b, int64_t p, int 
     // precision and rounded once (FP64 for complex128; hi/lo FP32 split of the
     // FP64 value for complex64).  Replaces the L x L per-rank tables of
     // init_forward_twiddles / init_inverse_twiddles (fft.cu:37-73).
+    // Also, for the size-specialised passes: w_N^{n1 k2} in [n1][k2] order (N
+    // entries) and the sub-transform tables w_VEC^m, w_M^m.  All four tables share one
+    // allocation of 16-byte entries.
+    P->twN = P->W = P->twv = P->twm = nullptr;
     if (flags & ZM_FLAG_HOST_ONLY) {
-        P->twN = nullptr;
         *plan = P;
         return ZM_OK;
     }
-    const size_t tw_bytes = (size_t)n * 16;
-    std::vector<unsigned char> host(tw_bytes);
+    const int64_t entries = 2 * n + g.vec + g.m;
+    std::vector<unsigned char> host((size_t)entries * 16);
     const long double pi = 3.141592653589793238462643383279502884L;
-    for (int64_t m = 0; m < n; m++) {
-        const long double th = -2.0L * pi * (long double)m / (long double)n;
+    auto put = [&](int64_t slot, int64_t m, int64_t len) {   // w_len^m
+        const long double th = -2.0L * pi * (long double)m / (long double)len;
         const double c = (double)cosl(th), s = (double)sinl(th);
         if (dtype == ZM_C128) {
-            double *d = reinterpret_cast<double *>(host.data()) + 2 * m;
+            double *d = reinterpret_cast<double *>(host.data()) + 2 * slot;
             d[0] = c; d[1] = s;
         } else {
-            float *f = reinterpret_cast<float *>(host.data()) + 4 * m;
+            float *f = reinterpret_cast<float *>(host.data()) + 4 * slot;
             const float ch = (float)c, sh = (float)s;
             f[0] = ch; f[1] = sh;
             f[2] = (float)(c - (double)ch); f[3] = (float)(s - (double)sh);
         }
-    }
-    cudaError_t e = cudaMalloc(&P->twN, tw_bytes);
+    };
+    for (int64_t m = 0; m < n; m++) put(m, m, n);
+    for (int64_t n1 = 0; n1 < g.m; n1++)
+        for (int64_t k2 = 0; k2 < g.vec; k2++) put(n + n1 * g.vec + k2, n1 * k2, n);
+    for (int64_t m = 0; m < g.vec; m++) put(2 * n + m, m, g.vec);
+    for (int64_t m = 0; m < g.m; m++) put(2 * n + g.vec + m, m, g.m);
+    void *tables = nullptr;
+    cudaError_t e = cudaMalloc(&tables, host.size());
     if (e != cudaSuccess) {
         delete P;
         return fail(ZM_ERR_NO_MEMORY, "twiddle table allocation failed: %s", cudaGetErrorString(e));
     }
-    e = cudaMemcpy(P->twN, host.data(), tw_bytes, cudaMemcpyHostToDevice);
+    e = cudaMemcpy(tables, host.data(), host.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
-        cudaFree(P->twN);
+        cudaFree(tables);
         delete P;
         return cuda_fail(e, "twiddle upload");
     }
+    unsigned char *tb = static_cast<unsigned char *>(tables);
+    P->twN = tb;
+    P->W = tb + (size_t)n * 16;
+    P->twv = tb + (size_t)2 * n * 16;
+    P->twm = tb + (size_t)(2 * n + g.vec) * 16;
     *plan = P;
     return ZM_OK;
 }

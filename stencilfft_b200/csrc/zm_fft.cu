@@ -22,69 +22,9 @@
 // the block synchronises, then every thread stores its results.
 #include "zm_common.cuh"
 #include "zm_internal.h"
+#include "zm_lines.cuh"
 
 namespace zm {
-
-// Addresses of a line on the vector side (A: chunk c, packed position
-// pos = j*VEC + n2, n1 = c*B + j) and on the frequency side (F: chunk
-// c = k2 / VP, position pos = k1*VP + k2 % VP).
-struct LineAddr {
-    int64_t a_base, a_chunk;
-    int64_t f_base, f_chunk, f_pos;
-};
-
-ZM_DEV LineAddr line_addr(const Geom &g, int kind, int64_t l) {
-    LineAddr a;
-    const int64_t L = g.L, P = g.p, LL = L * L, LLL = LL * L;
-    switch (kind) {
-    case PASS_X2: {  // line = (rid, q), q = packed position of local row lr
-        const int64_t rid = l >> g.logL, q = l & (L - 1);
-        const int64_t lr = unpack_pos(q, g.vec, g.logVEC, g.logB);
-        a.a_base = (rid * P) * LL + lr * L;       // rank (rid, 0), row lr
-        a.a_chunk = LL;                            // next cid
-        a.f_base = (rid * P) * LL + q;             // rank (rid, 0), column q (fft.cu:186)
-        a.f_chunk = LL;
-        a.f_pos = L;
-    } break;
-    case PASS_Y2: {  // line = (cid, p), p = x-frequency position (row after REPACK)
-        const int64_t cid = l >> g.logL, p = l & (L - 1);
-        a.a_base = cid * LL + p * L;               // rank (0, cid), row p
-        a.a_chunk = P * LL;                        // next rid
-        a.f_base = a.a_base;
-        a.f_chunk = a.a_chunk;
-        a.f_pos = 1;
-    } break;
-    case PASS_X3: {  // line = (did, rid, ld, q)
-        const int64_t q = l & (L - 1), ld = (l >> g.logL) & (L - 1), dr = l >> (2 * g.logL);
-        const int64_t lr = unpack_pos(q, g.vec, g.logVEC, g.logB);
-        a.a_base = dr * P * LLL + (ld * L + lr) * L;
-        a.a_chunk = LLL;
-        a.f_base = dr * P * LLL + ld * LL + q;     // repack_transpose_xy_3d (fft3d.cu:203-209)
-        a.f_chunk = LLL;
-        a.f_pos = L;
-    } break;
-    case PASS_Y3: {  // line = (did, cid, p, qd), qd = packed position of depth ld
-        const int64_t qd = l & (L - 1), p = (l >> g.logL) & (L - 1), dc = l >> (2 * g.logL);
-        const int64_t did = dc >> g.logP, cid = dc & (P - 1);
-        const int64_t ld = unpack_pos(qd, g.vec, g.logVEC, g.logB);
-        const int64_t r0 = did * P * P + cid;     // rank (did, 0, cid)
-        a.a_base = r0 * LLL + (ld * L + p) * L;
-        a.a_chunk = P * LLL;                       // next rid
-        a.f_base = r0 * LLL + p * L + qd;          // repack_transpose_yz_3d (fft3d.cu:214-220)
-        a.f_chunk = P * LLL;
-        a.f_pos = LL;
-    } break;
-    default: {       // PASS_Z3: line = (rid, cid, cy, rx)
-        const int64_t rc = l >> (2 * g.logL), rest = l & (LL - 1);
-        a.a_base = rc * LLL + rest * L;            // rank (0, rid, cid)
-        a.a_chunk = P * P * LLL;                   // next did
-        a.f_base = a.a_base;
-        a.f_chunk = a.a_chunk;
-        a.f_pos = 1;
-    } break;
-    }
-    return a;
-}
 
 // ------------------------------------------------------------ Stockham stage
 // One radix-R stage over all sub-transforms of length n held in shared memory.
@@ -299,6 +239,12 @@ static cudaError_t launch_typed(const LineParams &prm, int threads, size_t smem,
 int ept_for(int dtype) { return dtype == 0 ? 8 : 16; }
 
 cudaError_t launch_line_pass(const LineParams &prm, int dtype, bool inv, cudaStream_t st) {
+    if (!prm.permute_only && prm.W) {
+        bool handled = false;
+        cudaError_t e = dtype == 0 ? launch_fused_c128(prm, inv, st, &handled)
+                                   : launch_fused_c64(prm, inv, st, &handled);
+        if (handled) return e;
+    }
     const int ept = ept_for(dtype);
     const int threads = (int)((prm.T * prm.g.n) / ept);
     const size_t smem = (size_t)prm.T * prm.g.n * (dtype == 0 ? 16 : 8);

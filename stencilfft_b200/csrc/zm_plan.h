@@ -32,6 +32,9 @@ struct LineParams {
     const void *in;
     void *out;
     const void *twN;   // w_N^m, m < N, forward sign (tw<double> or tw<float>)
+    const void *W;     // w_N^{n1 k2} in [n1][k2] order (N entries)
+    const void *twv;   // w_VEC^m, m < VEC
+    const void *twm;   // w_M^m, m < M
     double scale_re, scale_im;
     int apply_scale;   // multiply the stored values by scale
     int permute_only;  // skip all arithmetic (reference do_compute=false)
@@ -50,6 +53,9 @@ struct zm_plan_s {
     size_t elem_bytes;
     int device;
     void *twN;        // device twiddle table (N entries)
+    void *W;          // w_N^{n1 k2}, [n1][k2] order (N entries)
+    void *twv;        // w_VEC^m (VEC entries)
+    void *twm;        // w_M^m (M entries)
     int T[3];         // lines per CTA for the passes (x, y, z)
     int max_radix;
 };

@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 # run.sh / run3d.sh sweep corners + small benchmark-shaped layouts
 CFG_2D = [(2, 64, 1, 2), (2, 64, 2, 2), (2, 64, 4, 2), (2, 64, 16, 2), (2, 64, 1, 4), (2, 64, 4, 4),
           (2, 128, 8, 4), (2, 256, 8, 2), (2, 256, 16, 4), (2, 512, 16, 2), (2, 1024, 32, 2),
-          (2, 1024, 64, 4)]
+          (2, 1024, 64, 4), (2, 512, 32, 4), (2, 2048, 32, 2), (2, 4096, 64, 4), (2, 4096, 32, 4)]
 CFG_3D = [(3, 16, 2, 2), (3, 16, 4, 2), (3, 32, 2, 4), (3, 32, 4, 2), (3, 64, 4, 4)]
 
 
