@@ -92,6 +92,15 @@ int zm_plan_destroy(zm_plan plan);   /* destroy_plans / destroy_buffers (fft_hos
 int zm_plan_get_info(zm_plan plan, zm_plan_info *info);
 /* Workspace a transform needs to leave its input untouched (one field, or 0). */
 int zm_plan_workspace_size(zm_plan plan, size_t *bytes);
+/*
+ * Tile shapes of the fused FFT pass (no counterpart in the reference; the autotuner's
+ * knob next to B_DIM): the number of size-specialised variants for this plan's
+ * (VEC, M, dtype) -- cluster size, lines per tile, threads -- and the one to use
+ * (0 = default).  Results do not depend on the variant beyond rounding.  Set it before
+ * the plan is used, not while calls using the plan are in flight.
+ */
+int zm_plan_kernel_variants(zm_plan plan, int *count);
+int zm_plan_set_kernel_variant(zm_plan plan, int variant);
 
 /*
  * Transforms over all virtual ranks.

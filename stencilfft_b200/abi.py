@@ -56,6 +56,8 @@ SIGNATURES = {
     "zm_plan_destroy": [_P],
     "zm_plan_get_info": [_P, ctypes.POINTER(zm_plan_info)],
     "zm_plan_workspace_size": [_P, ctypes.POINTER(ctypes.c_size_t)],
+    "zm_plan_kernel_variants": [_P, ctypes.POINTER(ctypes.c_int)],
+    "zm_plan_set_kernel_variant": [_P, ctypes.c_int],
     "zm_fft_forward": [_P, _P, _P, _P, _P],
     "zm_fft_inverse": [_P, _P, _P, _P, _D, _D, _P],
     "zm_fft_inverse_static": [_P, _P, _P, _D, _D, _P],

@@ -1,0 +1,43 @@
+"""Generates zm_fft2_<dtype>_<dir>.cu: the size-specialised fused passes and their
+dispatch tables.  Each (log2 VEC, log2 M) pair lists variants (cluster size CL, lines
+per tile TL, threads NT); the plan's `variant` picks one (0 = default)."""
+VARIANTS = {
+    "c64": {
+        (4, 4): [(1, 32, 512)], (4, 5): [(1, 16, 512)], (4, 6): [(1, 8, 512), (1, 4, 256)],
+        (2, 7): [(1, 16, 512)], (5, 6): [(1, 4, 512)],
+        (5, 7): [(1, 2, 512), (2, 2, 256), (2, 4, 512)],
+        (4, 8): [(1, 2, 512), (2, 4, 512)],
+        (5, 8): [(2, 2, 512), (1, 1, 512), (2, 1, 256)],
+        (6, 7): [(1, 1, 512), (2, 2, 512)],
+        (6, 8): [(2, 1, 512), (4, 2, 512), (1, 1, 1024)],
+    },
+    "c128": {
+        (4, 4): [(1, 16, 256)], (4, 5): [(1, 8, 256)], (4, 6): [(1, 4, 256)], (2, 7): [(1, 8, 256)],
+        (5, 6): [(1, 2, 256)], (5, 7): [(1, 1, 256), (2, 2, 256)], (4, 8): [(1, 1, 256), (2, 2, 256)],
+        (5, 8): [(2, 1, 256), (1, 1, 512)], (6, 7): [(2, 1, 256), (1, 1, 512)],
+        (6, 8): [(4, 1, 256), (2, 1, 512), (4, 2, 512)],
+    },
+}
+T = {"c64": "float", "c128": "double"}
+for dt, table in VARIANTS.items():
+    for inv in (False, True):
+        d = "inv" if inv else "fwd"
+        L = [f"// zm_fft2_{dt}_{d}.cu -- generated by gen_fused.py: size-specialised fused axis passes,",
+             f"// {dt}, {'inverse' if inv else 'forward'} direction (kernel template in zm_fft2.cuh).",
+             '#include "zm_internal.h"', '#include "zm_lines.cuh"', '#include "zm_fft2.cuh"', "",
+             "namespace zm {", "",
+             f"cudaError_t launch_fused_{dt}_{d}(const LineParams &prm, cudaStream_t st, bool *handled) {{",
+             "    *handled = true;",
+             "    switch ((prm.g.logVEC << 16) | (prm.g.logM << 8) | prm.variant) {"]
+        for (lv, lm), vs in table.items():
+            for vi, (cl, tl, nt) in enumerate(vs):
+                L.append(f"    case ({lv} << 16) | ({lm} << 8) | {vi}: "
+                         f"return launch_fused<{T[dt]}, {lv}, {lm}, {cl}, {tl}, {nt}>(prm, {'true' if inv else 'false'}, st);")
+        L += ["    default: break;", "    }", "    *handled = false;", "    return cudaSuccess;", "}", ""]
+        if not inv:
+            L += [f"int fused_variants_{dt}(int logvec, int logm) {{", "    switch ((logvec << 8) | logm) {"]
+            for (lv, lm), vs in table.items():
+                L.append(f"    case ({lv} << 8) | {lm}: return {len(vs)};")
+            L += ["    default: return 0;", "    }", "}", ""]
+        L += ["}  // namespace zm", ""]
+        open(f"zm_fft2_{dt}_{d}.cu", "w").write("\n".join(L))

@@ -129,9 +129,7 @@ static int pick_lines(const zm_plan_s *p) {
 
 static bool fft_supported(const zm_plan_s *p, std::string *why) {
     const bool permute = (p->flags & ZM_FLAG_PERMUTE_ONLY) != 0;
-    const int fused = p->dtype == ZM_C128 ? zm::fused_lines_c128(p->g.logVEC, p->g.logM)
-                                          : zm::fused_lines_c64(p->g.logVEC, p->g.logM);
-    if (fused > 0 && !permute) return true;
+    if (p->nvariants > 0 && !permute) return true;
     const int ept = zm::ept_for(p->dtype);
     const int64_t threads = (int64_t)p->T[0] * p->g.n / ept;
     const int64_t smem = (int64_t)p->T[0] * p->g.n * (int64_t)p->elem_bytes;
@@ -157,6 +155,7 @@ static LineParams line_params(const zm_plan_s *p, int kind, const void *in, void
     lp.scale_re = 1.0;
     lp.scale_im = 0.0;
     lp.apply_scale = 0;
+    lp.variant = p->variant;
     lp.permute_only = (p->flags & ZM_FLAG_PERMUTE_ONLY) ? 1 : 0;
     lp.nst_vec = schedule(p->g.vec, p->max_radix, lp.rad_vec);
     lp.nst_m = schedule(p->g.m, p->max_radix, lp.rad_m);
@@ -266,6 +265,9 @@ int zm_plan_create(zm_plan *plan, int dim, int64_t n, int64_t b, int64_t p, int 
     cudaGetDevice(&P->device);
     const int t = pick_lines(P);
     P->T[0] = P->T[1] = P->T[2] = t;
+    P->variant = 0;
+    P->nvariants = dtype == ZM_C128 ? zm::fused_variants_c128(g.logVEC, g.logM)
+                                    : zm::fused_variants_c64(g.logVEC, g.logM);
 
     // Twiddle table w_N^m = exp(-2 pi i m / N), m < N, generated in extended
     // precision and rounded once (FP64 for complex128; hi/lo FP32 split of the
@@ -325,6 +327,24 @@ int zm_plan_destroy(zm_plan plan) {
     if (!plan) return fail(ZM_ERR_INVALID_ARG, "null plan");
     if (plan->twN) cudaFree(plan->twN);
     delete plan;
+    return ZM_OK;
+}
+
+int zm_plan_kernel_variants(zm_plan plan, int *count) {
+    int rc;
+    if ((rc = check_plan(plan))) return rc;
+    if (!count) return fail(ZM_ERR_INVALID_ARG, "count is NULL");
+    *count = plan->nvariants;
+    return ZM_OK;
+}
+
+int zm_plan_set_kernel_variant(zm_plan plan, int variant) {
+    int rc;
+    if ((rc = check_plan(plan))) return rc;
+    if (variant < 0 || (variant > 0 && variant >= plan->nvariants))
+        return fail(ZM_ERR_INVALID_ARG, "variant %d out of range (%d available)", variant,
+                    plan->nvariants);
+    plan->variant = variant;
     return ZM_OK;
 }
 

@@ -241,8 +241,9 @@ int ept_for(int dtype) { return dtype == 0 ? 8 : 16; }
 cudaError_t launch_line_pass(const LineParams &prm, int dtype, bool inv, cudaStream_t st) {
     if (!prm.permute_only && prm.W) {
         bool handled = false;
-        cudaError_t e = dtype == 0 ? launch_fused_c128(prm, inv, st, &handled)
-                                   : launch_fused_c64(prm, inv, st, &handled);
+        cudaError_t e;
+        if (dtype == 0) e = inv ? launch_fused_c128_inv(prm, st, &handled) : launch_fused_c128_fwd(prm, st, &handled);
+        else e = inv ? launch_fused_c64_inv(prm, st, &handled) : launch_fused_c64_fwd(prm, st, &handled);
         if (handled) return e;
     }
     const int ept = ept_for(dtype);

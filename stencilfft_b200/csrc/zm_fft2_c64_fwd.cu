@@ -1,0 +1,53 @@
+// zm_fft2_c64_fwd.cu -- generated by gen_fused.py: size-specialised fused axis passes,
+// c64, forward direction (kernel template in zm_fft2.cuh).
+#include "zm_internal.h"
+#include "zm_lines.cuh"
+#include "zm_fft2.cuh"
+
+namespace zm {
+
+cudaError_t launch_fused_c64_fwd(const LineParams &prm, cudaStream_t st, bool *handled) {
+    *handled = true;
+    switch ((prm.g.logVEC << 16) | (prm.g.logM << 8) | prm.variant) {
+    case (4 << 16) | (4 << 8) | 0: return launch_fused<float, 4, 4, 1, 32, 512>(prm, false, st);
+    case (4 << 16) | (5 << 8) | 0: return launch_fused<float, 4, 5, 1, 16, 512>(prm, false, st);
+    case (4 << 16) | (6 << 8) | 0: return launch_fused<float, 4, 6, 1, 8, 512>(prm, false, st);
+    case (4 << 16) | (6 << 8) | 1: return launch_fused<float, 4, 6, 1, 4, 256>(prm, false, st);
+    case (2 << 16) | (7 << 8) | 0: return launch_fused<float, 2, 7, 1, 16, 512>(prm, false, st);
+    case (5 << 16) | (6 << 8) | 0: return launch_fused<float, 5, 6, 1, 4, 512>(prm, false, st);
+    case (5 << 16) | (7 << 8) | 0: return launch_fused<float, 5, 7, 1, 2, 512>(prm, false, st);
+    case (5 << 16) | (7 << 8) | 1: return launch_fused<float, 5, 7, 2, 2, 256>(prm, false, st);
+    case (5 << 16) | (7 << 8) | 2: return launch_fused<float, 5, 7, 2, 4, 512>(prm, false, st);
+    case (4 << 16) | (8 << 8) | 0: return launch_fused<float, 4, 8, 1, 2, 512>(prm, false, st);
+    case (4 << 16) | (8 << 8) | 1: return launch_fused<float, 4, 8, 2, 4, 512>(prm, false, st);
+    case (5 << 16) | (8 << 8) | 0: return launch_fused<float, 5, 8, 2, 2, 512>(prm, false, st);
+    case (5 << 16) | (8 << 8) | 1: return launch_fused<float, 5, 8, 1, 1, 512>(prm, false, st);
+    case (5 << 16) | (8 << 8) | 2: return launch_fused<float, 5, 8, 2, 1, 256>(prm, false, st);
+    case (6 << 16) | (7 << 8) | 0: return launch_fused<float, 6, 7, 1, 1, 512>(prm, false, st);
+    case (6 << 16) | (7 << 8) | 1: return launch_fused<float, 6, 7, 2, 2, 512>(prm, false, st);
+    case (6 << 16) | (8 << 8) | 0: return launch_fused<float, 6, 8, 2, 1, 512>(prm, false, st);
+    case (6 << 16) | (8 << 8) | 1: return launch_fused<float, 6, 8, 4, 2, 512>(prm, false, st);
+    case (6 << 16) | (8 << 8) | 2: return launch_fused<float, 6, 8, 1, 1, 1024>(prm, false, st);
+    default: break;
+    }
+    *handled = false;
+    return cudaSuccess;
+}
+
+int fused_variants_c64(int logvec, int logm) {
+    switch ((logvec << 8) | logm) {
+    case (4 << 8) | 4: return 1;
+    case (4 << 8) | 5: return 1;
+    case (4 << 8) | 6: return 2;
+    case (2 << 8) | 7: return 1;
+    case (5 << 8) | 6: return 1;
+    case (5 << 8) | 7: return 3;
+    case (4 << 8) | 8: return 2;
+    case (5 << 8) | 8: return 3;
+    case (6 << 8) | 7: return 2;
+    case (6 << 8) | 8: return 3;
+    default: return 0;
+    }
+}
+
+}  // namespace zm

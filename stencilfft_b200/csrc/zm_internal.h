@@ -17,13 +17,15 @@ int report_error(int code, const char *fmt, ...);
 int ept_for(int dtype);
 cudaError_t launch_line_pass(const LineParams &prm, int dtype, bool inv, cudaStream_t st);
 
-// zm_fft2_c64.cu / zm_fft2_c128.cu: size-specialised fused passes.  `handled` is false
-// when (log2 VEC, log2 M) has no specialisation; fused_lines_* gives its lines per CTA
-// (0 = none).
-cudaError_t launch_fused_c64(const LineParams &prm, bool inv, cudaStream_t st, bool *handled);
-cudaError_t launch_fused_c128(const LineParams &prm, bool inv, cudaStream_t st, bool *handled);
-int fused_lines_c64(int logvec, int logm);
-int fused_lines_c128(int logvec, int logm);
+// zm_fft2_<dtype>_<dir>.cu (generated by gen_fused.py): size-specialised fused passes.
+// `handled` is false when (log2 VEC, log2 M, variant) has no specialisation;
+// fused_variants_* gives the number of tile-shape variants (0 = none).
+cudaError_t launch_fused_c64_fwd(const LineParams &prm, cudaStream_t st, bool *handled);
+cudaError_t launch_fused_c64_inv(const LineParams &prm, cudaStream_t st, bool *handled);
+cudaError_t launch_fused_c128_fwd(const LineParams &prm, cudaStream_t st, bool *handled);
+cudaError_t launch_fused_c128_inv(const LineParams &prm, cudaStream_t st, bool *handled);
+int fused_variants_c64(int logvec, int logm);
+int fused_variants_c128(int logvec, int logm);
 
 // zm_stencil.cu
 enum StencilOp : int { ST_LAPLACE = 0, ST_DX = 1, ST_DY = 2 };

@@ -37,6 +37,7 @@ struct LineParams {
     const void *twm;   // w_M^m, m < M
     double scale_re, scale_im;
     int apply_scale;   // multiply the stored values by scale
+    int variant;       // tile-shape variant of the size-specialised kernel (0 = default)
     int permute_only;  // skip all arithmetic (reference do_compute=false)
     // radix schedules of the two sub-transforms (first stage first)
     int nst_vec, nst_m;
@@ -58,4 +59,6 @@ struct zm_plan_s {
     void *twm;        // w_M^m (M entries)
     int T[3];         // lines per CTA for the passes (x, y, z)
     int max_radix;
+    int variant;      // tile-shape variant of the size-specialised kernel
+    int nvariants;    // variants available for (VEC, M, dtype); 0 = runtime-sized kernel only
 };

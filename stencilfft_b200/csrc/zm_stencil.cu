@@ -5,39 +5,40 @@
 // (communicate_laplace, laplace.cu:194-256) and then runs a one-element-per-
 // thread kernel that picks each neighbour from its own array or a receive
 // buffer (laplace.cu:73-169).  With every virtual rank in one HBM the halo is
-// simply the neighbouring rank's array: each thread maps its element to global
+// simply the neighbouring rank's array: each thread maps its elements to global
 // (row, column[, depth]) coordinates, steps one (two) points along the axis
 // with periodic wrap, and maps back to (rank, local row, packed column) with the
 // block-cyclic maps of zmodel/utils.h:166-214.  The neighbours are accumulated
 // in the reference's order (above, below, left, right[, front, back], then the
 // centre term), so the 2D Laplacian and dx / dy are bit-identical to it in FP64.
+//
+// Each thread handles one 16-byte vector of the field (two complex64, one
+// complex128, four float or two double values).  The elements of a vector share a
+// row and a packed vector j, so every neighbour along y or z is again one aligned
+// 16-byte vector; along x it is one too except where the step crosses into the
+// left / right rank at the periodic wrap (utils.h:122-128: the shift by one
+// element at cid = 0 / P-1), which is read element by element.
 #include "zm_common.cuh"
 #include "zm_internal.h"
 
 namespace zm {
 
-struct StencilGeom {
-    Geom g;
-    int64_t total;   // elements in the field
-    int threads_per_elem_shift;
-};
-
 // global row/column/depth coordinate of a local (block-cyclic) index, and back
-ZM_DEV int64_t l2g(int64_t li, int64_t id, const Geom &g) {   // utils.h:168
-    return ((li >> g.logB) << (g.logB + g.logP)) + (id << g.logB) + (li & (g.b - 1));
+ZM_DEV int l2g(int li, int id, const Geom &g) {   // utils.h:168
+    return ((li >> g.logB) << (g.logB + g.logP)) + (id << g.logB) + (li & ((int)g.b - 1));
 }
-ZM_DEV void g2l(int64_t gi, const Geom &g, int64_t &id, int64_t &li) {  // utils.h:178-180
-    id = (gi >> g.logB) & (g.p - 1);
-    li = ((gi >> (g.logB + g.logP)) << g.logB) + (gi & (g.b - 1));
+ZM_DEV void g2l(int gi, const Geom &g, int &id, int &li) {  // utils.h:178-180
+    id = (gi >> g.logB) & ((int)g.p - 1);
+    li = ((gi >> (g.logB + g.logP)) << g.logB) + (gi & ((int)g.b - 1));
 }
 // packed column position <-> global column (utils.h:122-128 then 169)
-ZM_DEV int64_t pos2gc(int64_t pos, int64_t cid, const Geom &g) {
-    const int64_t j = pos >> g.logVEC, jj = pos & (g.vec - 1);
+ZM_DEV int pos2gc(int pos, int cid, const Geom &g) {
+    const int j = pos >> g.logVEC, jj = pos & ((int)g.vec - 1);
     return (jj << (g.logB + g.logP)) + (cid << g.logB) + j;
 }
-ZM_DEV void gc2pos(int64_t gc, const Geom &g, int64_t &cid, int64_t &pos) {
-    cid = (gc >> g.logB) & (g.p - 1);
-    pos = ((gc & (g.b - 1)) << g.logVEC) + (gc >> (g.logB + g.logP));
+ZM_DEV void gc2pos(int gc, const Geom &g, int &cid, int &pos) {
+    cid = (gc >> g.logB) & ((int)g.p - 1);
+    pos = ((gc & ((int)g.b - 1)) << g.logVEC) + (gc >> (g.logB + g.logP));
 }
 
 template <typename V> struct ops;
@@ -56,102 +57,161 @@ template <> struct ops<float> {
     static ZM_DEV float div(float a, float b) { return __fdiv_rn(a, b); }
 };
 
-// NC = scalar components per element (2 complex, 1 real); S = scalar type.
+// 16 bytes of scalars
+template <typename S> struct vec16 {
+    static constexpr int n = 16 / (int)sizeof(S);
+    S v[n];
+};
+
+// S = scalar type; NC = scalars per element (2 complex, 1 real).  One thread = one
+// 16-byte vector = K = 16 / (NC * sizeof(S)) consecutive elements.
 template <typename S, int NC, int OP, int DIM>
 __global__ void __launch_bounds__(256) stencil_kernel(const S *__restrict__ in, S *__restrict__ out,
-                                                      const Geom g, int64_t total, S coef) {
+                                                      const Geom g, int64_t nvec, S coef) {
     using O = ops<S>;
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= total) return;
-    const int64_t L = g.L, LL = L * L;
-    const int64_t N = g.n;
-    int64_t rank, lr, ld = 0, pos, rid, cid, did = 0;
+    using V = vec16<S>;
+    constexpr int K = V::n / NC;                 // elements per vector
+    const int64_t vi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (vi >= nvec) return;
+    const int64_t e = vi * K;                    // first element
+    const int L = (int)g.L;
+    const int N = (int)g.n;
+    int rank, lr, ld = 0, did = 0;
     if (DIM == 2) {
-        rank = e >> (2 * g.logL);
-        lr = (e >> g.logL) & (L - 1);
-        rid = rank >> g.logP;
-        cid = rank & (g.p - 1);
+        rank = (int)(e >> (2 * g.logL));
+        lr = (int)(e >> g.logL) & (L - 1);
     } else {
-        rank = e >> (3 * g.logL);
-        ld = (e >> (2 * g.logL)) & (L - 1);
-        lr = (e >> g.logL) & (L - 1);
-        did = rank >> (2 * g.logP);
-        rid = (rank >> g.logP) & (g.p - 1);
-        cid = rank & (g.p - 1);
+        rank = (int)(e >> (3 * g.logL));
+        ld = (int)(e >> (2 * g.logL)) & (L - 1);
+        lr = (int)(e >> g.logL) & (L - 1);
     }
-    pos = e & (L - 1);
-    const int64_t gr = l2g(lr, rid, g);
-    const int64_t gc = pos2gc(pos, cid, g);
-    const int64_t gd = DIM == 3 ? l2g(ld, did, g) : 0;
-    const int64_t P = g.p;
-    auto rank_of = [&](int64_t d_, int64_t r_, int64_t c_) {
-        return DIM == 2 ? r_ * P + c_ : (d_ * P + r_) * P + c_;
+    const int pos = (int)(e & (L - 1));
+    const int P = (int)g.p;
+    const int cid = rank & (P - 1);
+    const int rid = DIM == 2 ? rank >> g.logP : (rank >> g.logP) & (P - 1);
+    if (DIM == 3) did = rank >> (2 * g.logP);
+    const int gr = l2g(lr, rid, g);
+    const int gd = DIM == 3 ? l2g(ld, did, g) : 0;
+    auto rank_of = [&](int d_, int r_, int c_) { return DIM == 2 ? r_ * P + c_ : (d_ * P + r_) * P + c_; };
+    auto addr = [&](int rk, int ld_, int lr_, int pos_) -> int64_t {
+        return DIM == 2 ? ((int64_t)rk << (2 * g.logL)) + (int64_t)lr_ * L + pos_
+                        : ((int64_t)rk << (3 * g.logL)) + ((int64_t)ld_ * L + lr_) * L + pos_;
     };
-    auto addr = [&](int64_t rk, int64_t ld_, int64_t lr_, int64_t pos_) {
-        return DIM == 2 ? (rk << (2 * g.logL)) + lr_ * L + pos_
-                        : (rk << (3 * g.logL)) + ld_ * LL + lr_ * L + pos_;
-    };
-    // neighbour along rows (y) at global row gr + d
-    auto nb_row = [&](int64_t d) {
-        int64_t id, li;
+    // neighbour vectors along y (rows) and z (depth): same packed position
+    auto vrow = [&](int d) {
+        int id, li;
         g2l((gr + d + N) & (N - 1), g, id, li);
-        return addr(rank_of(did, id, cid), ld, li, pos);
+        return __ldg(reinterpret_cast<const uint4 *>(in + addr(rank_of(did, id, cid), ld, li, pos) * NC));
     };
-    auto nb_col = [&](int64_t d) {
-        int64_t id, ps;
-        gc2pos((gc + d + N) & (N - 1), g, id, ps);
-        return addr(rank_of(did, rid, id), ld, lr, ps);
-    };
-    auto nb_dep = [&](int64_t d) {
-        int64_t id, li;
+    auto vdep = [&](int d) {
+        int id, li;
         g2l((gd + d + N) & (N - 1), g, id, li);
-        return addr(rank_of(id, rid, cid), li, lr, pos);
+        return __ldg(reinterpret_cast<const uint4 *>(in + addr(rank_of(id, rid, cid), li, lr, pos) * NC));
     };
-#pragma unroll
-    for (int q = 0; q < NC; q++) {
-        auto ld_ = [&](int64_t a) { return __ldg(in + a * NC + q); };
-        S res;
-        if (OP == ST_LAPLACE) {
-            // laplace.cu:91-168 / laplace3d.cu:98-224 accumulation order
-            S s = O::add((S)0, ld_(nb_row(-1)));   // scratch = {0,0}; scratch += above
-            s = O::add(s, ld_(nb_row(1)));
-            s = O::add(s, ld_(nb_col(-1)));
-            s = O::add(s, ld_(nb_col(1)));
-            if (DIM == 3) {
-                s = O::add(s, ld_(nb_dep(-1)));
-                s = O::add(s, ld_(nb_dep(1)));
-            }
-            s = O::fmaop((S)(-2 * DIM), ld_(e), s);
-            res = O::mul(s, coef);       // coef = 1/h^2 (1 reproduces the reference)
-        } else {
-            // dx.cu:26-79 / dy.cu:34-100: ((-8 f[-1] + f[-2]) + 8 f[+1]) - f[+2], then / (12 delta)
-            auto nb = [&](int64_t d) { return OP == ST_DX ? nb_col(d) : nb_row(d); };
-            S s = O::add((S)0, O::mul(ld_(nb(-1)), (S)-8));
-            s = O::add(s, ld_(nb(-2)));
-            s = O::add(s, O::mul(ld_(nb(1)), (S)8));
-            s = O::sub(s, ld_(nb(2)));
-            res = O::div(s, O::mul((S)12, coef));   // coef = delta
+    // neighbour along x (columns) at column offset d of the K elements
+    auto vcol = [&](int d) {
+        V r;
+        const int j = pos >> g.logVEC;
+        if (j + d >= 0 && j + d < (int)g.b && (K == 1 || (int)g.vec % K == 0)) {
+            // same rank and same jj: the neighbour vector is d packed vectors away
+            *reinterpret_cast<uint4 *>(&r) = __ldg(reinterpret_cast<const uint4 *>(
+                in + (e + (int64_t)d * (int64_t)g.vec) * NC));
+            return r;
         }
-        out[e * NC + q] = res;
+        const int gc0 = pos2gc(pos, cid, g);
+        int id0, p0;
+        gc2pos((gc0 + d + N) & (N - 1), g, id0, p0);
+        const int64_t a0 = addr(rank_of(did, rid, id0), ld, lr, p0);
+        bool contiguous = true;
+        if (K > 1) {
+            const int gcl = pos2gc(pos + K - 1, cid, g);
+            int idl, pl;
+            gc2pos((gcl + d + N) & (N - 1), g, idl, pl);
+            // one aligned 16-byte load only if the K neighbours are consecutive and start on
+            // a K-element boundary (the cid = 0 wrap shifts them by one element)
+            contiguous = idl == id0 && pl == p0 + K - 1 && (p0 & (K - 1)) == 0;
+        }
+        if (contiguous) {
+            *reinterpret_cast<uint4 *>(&r) = __ldg(reinterpret_cast<const uint4 *>(in + a0 * NC));
+        } else {
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                int idk, pk;
+                gc2pos((pos2gc(pos + k, cid, g) + d + N) & (N - 1), g, idk, pk);
+                const int64_t ak = addr(rank_of(did, rid, idk), ld, lr, pk);
+#pragma unroll
+                for (int q = 0; q < NC; q++) r.v[k * NC + q] = __ldg(in + ak * NC + q);
+            }
+        }
+        return r;
+    };
+    auto as = [](uint4 u) {
+        V r;
+        *reinterpret_cast<uint4 *>(&r) = u;
+        return r;
+    };
+    V res;
+    if (OP == ST_LAPLACE) {
+        // laplace.cu:91-168 / laplace3d.cu:98-224 accumulation order
+        const V up = as(vrow(-1)), dn = as(vrow(1)), lf = vcol(-1), rt = vcol(1);
+        const V c = as(__ldg(reinterpret_cast<const uint4 *>(in + e * NC)));
+        V fr, bk;
+        if (DIM == 3) {
+            fr = as(vdep(-1));
+            bk = as(vdep(1));
+        }
+#pragma unroll
+        for (int i = 0; i < V::n; i++) {
+            S s = O::add((S)0, up.v[i]);      // scratch = {0,0}; scratch += above
+            s = O::add(s, dn.v[i]);
+            s = O::add(s, lf.v[i]);
+            s = O::add(s, rt.v[i]);
+            if (DIM == 3) {
+                s = O::add(s, fr.v[i]);
+                s = O::add(s, bk.v[i]);
+            }
+            s = O::fmaop((S)(-2 * DIM), c.v[i], s);
+            res.v[i] = O::mul(s, coef);       // coef = 1/h^2 (1 reproduces the reference)
+        }
+    } else {
+        // dx.cu:26-79 / dy.cu:34-100: ((-8 f[-1] + f[-2]) + 8 f[+1]) - f[+2], then / (12 delta)
+        V m1, m2, p1, p2;
+        if (OP == ST_DX) {
+            m1 = vcol(-1); m2 = vcol(-2); p1 = vcol(1); p2 = vcol(2);
+        } else {
+            m1 = as(vrow(-1)); m2 = as(vrow(-2)); p1 = as(vrow(1)); p2 = as(vrow(2));
+        }
+        const S den = O::mul((S)12, coef);    // coef = delta
+#pragma unroll
+        for (int i = 0; i < V::n; i++) {
+            S s = O::add((S)0, O::mul(m1.v[i], (S)-8));
+            s = O::add(s, m2.v[i]);
+            s = O::add(s, O::mul(p1.v[i], (S)8));
+            s = O::sub(s, p2.v[i]);
+            res.v[i] = O::div(s, den);
+        }
     }
+    *reinterpret_cast<uint4 *>(out + e * NC) = *reinterpret_cast<const uint4 *>(&res);
 }
 
 template <typename S, int NC>
 static cudaError_t launch_s(const zm_plan_s *p, int op, const void *in, void *out, double coef,
                             cudaStream_t st) {
-    const int64_t total = p->total;
+    constexpr int K = 16 / (int)sizeof(S) / NC;
+    if (p->g.L % K) return cudaErrorInvalidValue;
+    const int64_t nvec = p->total / K;
     const int threads = 256;
-    const unsigned grid = (unsigned)((total + threads - 1) / threads);
+    const unsigned grid = (unsigned)((nvec + threads - 1) / threads);
     const S *i = reinterpret_cast<const S *>(in);
     S *o = reinterpret_cast<S *>(out);
     const S c = (S)coef;
     if (p->g.dim == 2) {
-        if (op == ST_LAPLACE) stencil_kernel<S, NC, ST_LAPLACE, 2><<<grid, threads, 0, st>>>(i, o, p->g, total, c);
-        else if (op == ST_DX) stencil_kernel<S, NC, ST_DX, 2><<<grid, threads, 0, st>>>(i, o, p->g, total, c);
-        else stencil_kernel<S, NC, ST_DY, 2><<<grid, threads, 0, st>>>(i, o, p->g, total, c);
+        if (op == ST_LAPLACE) stencil_kernel<S, NC, ST_LAPLACE, 2><<<grid, threads, 0, st>>>(i, o, p->g, nvec, c);
+        else if (op == ST_DX) stencil_kernel<S, NC, ST_DX, 2><<<grid, threads, 0, st>>>(i, o, p->g, nvec, c);
+        else stencil_kernel<S, NC, ST_DY, 2><<<grid, threads, 0, st>>>(i, o, p->g, nvec, c);
     } else {
         if (op != ST_LAPLACE) return cudaErrorInvalidValue;
-        stencil_kernel<S, NC, ST_LAPLACE, 3><<<grid, threads, 0, st>>>(i, o, p->g, total, c);
+        stencil_kernel<S, NC, ST_LAPLACE, 3><<<grid, threads, 0, st>>>(i, o, p->g, nvec, c);
     }
     count_launch();
     return cudaGetLastError();

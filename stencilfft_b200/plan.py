@@ -96,6 +96,16 @@ class Plan:
         if t.numel() != self.total or not t.is_contiguous():
             raise ValueError(f"{name} must be a contiguous tensor of {self.total} elements")
 
+    # ------------------------------------------------------------ tuning
+    @property
+    def kernel_variants(self) -> int:
+        n = ctypes.c_int()
+        check(lib().zm_plan_kernel_variants(self._h, ctypes.byref(n)), "zm_plan_kernel_variants")
+        return n.value
+
+    def set_kernel_variant(self, variant: int) -> None:
+        check(lib().zm_plan_set_kernel_variant(self._h, int(variant)), "zm_plan_set_kernel_variant")
+
     # ------------------------------------------------------------ transforms
     def forward_fft(self, buf0, buf1, work=None, stream=None):
         """forward_fft / forward_fft_3d: real layout buf0 -> reciprocal layout buf1."""

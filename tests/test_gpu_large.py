@@ -41,6 +41,34 @@ def test_plane_waves_give_spikes(n, b, p, dt):
     assert err < (1e-12 if dt == "c128" else 1e-6), err
 
 
+@pytest.mark.parametrize("n,b,p,dt", [(16384, 64, 4, "c64"), (16384, 64, 4, "c128"),
+                                      (8192, 64, 4, "c64"), (8192, 32, 4, "c128")])
+def test_every_kernel_variant_full_size(n, b, p, dt):
+    """Every tile shape (cluster size, lines per tile) at full size: plane-wave spikes and
+    identical results across variants."""
+    import torch
+    from stencilfft_b200 import Plan
+    pl = Plan(2, n, b, p, dtype=dt)
+    modes = np.array([[5, -9], [n // 4 - 3, n // 8 + 1], [-(n // 8), 3]], dtype=np.int64)
+    amps = np.array([[1.0, -1.0], [0.5, 0.25], [-2.0, 0.0]])
+    u = pl.empty()
+    pl.fill_modes(u, modes, amps, 0.0, 0)
+    nat = torch.zeros(n * n, dtype=pl.torch_dtype, device="cuda")
+    for (kx, ky), (ar, ai) in zip(modes, amps):
+        nat[(ky % n) * n + (kx % n)] += complex(ar, ai) * n * n
+    exp = pl.empty()
+    pl.natural_to_reciprocal(nat, exp)
+    del nat
+    spec, work, back = pl.empty(), pl.empty(), pl.empty()
+    tol = 1e-12 if dt == "c128" else 1e-6
+    for v in range(pl.kernel_variants):
+        pl.set_kernel_variant(v)
+        pl.forward_fft(u, spec, work=work)
+        assert _norm(spec - exp) / _norm(exp) < tol, v
+        pl.inverse_fft(spec, back, scale=1.0 / (n * n), work=work)
+        assert _norm(back - u) / _norm(u) < tol, v
+
+
 @pytest.mark.parametrize("n,b,p,dt", LARGE)
 def test_round_trip(n, b, p, dt):
     import torch

@@ -47,6 +47,26 @@ def test_forward_inverse_match_oracle(dim, n, b, p, dt):
     assert relerr(to_host(back), buf) < TOL[dt]
 
 
+@pytest.mark.parametrize("dt", ["c128", "c64"])
+@pytest.mark.parametrize("dim,n,b,p", [(2, 4096, 32, 4), (2, 4096, 64, 4), (2, 1024, 32, 2)])
+def test_every_kernel_variant_matches_oracle(dim, n, b, p, dt):
+    """Each tile shape of the fused pass (cluster size, lines per tile) gives the same transform."""
+    import torch
+    x = rand_field(dim, n, seed=17)
+    buf = O.natural_to_real_layout(x, b, p)
+    ref = O.forward_fft(buf, dim, n, b, p)
+    pl = _plan(dim, n, b, p, dt)
+    assert pl.kernel_variants >= 1
+    d_in = to_dev(buf, dt)
+    d_out, work, back = torch.empty_like(d_in), torch.empty_like(d_in), torch.empty_like(d_in)
+    for v in range(pl.kernel_variants):
+        pl.set_kernel_variant(v)
+        pl.forward_fft(d_in, d_out, work=work)
+        assert relerr(to_host(d_out), ref) < TOL[dt], v
+        pl.inverse_fft(d_out, back, scale=1.0 / n ** dim, work=work)
+        assert relerr(to_host(back), buf) < TOL[dt], v
+
+
 @pytest.mark.parametrize("dim,n,b,p", CFG_2D[:6] + CFG_3D[:3])
 def test_reference_contract_buf0_clobbered(dim, n, b, p):
     """work=None: buf0 may be used as scratch (fft.cu:189-198); results unchanged."""
