@@ -336,6 +336,15 @@ def run_profile_case(args):
     modes, amps = modes_and_amps(n)
     u = pl.empty()
     pl.fill_modes(u, modes, amps, NOISE, NOISE_SEED)
+    if args.profile_ops == "fwd":
+        # forward transform only: two buffers on the device
+        spec = pl.empty()
+        for _ in range(2):
+            pl.forward_fft(u, spec)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": {"n": n, "p": P, "b": B, "dtype": args.profile_dtype,
+                                           "ops": "fwd", "field_bytes": pl.field_bytes}}))
+        return
     spec, back, work, out = pl.empty(), pl.empty(), pl.empty(), pl.empty()
     for _ in range(2):
         pl.forward_fft(u, spec, work=work)
@@ -359,6 +368,7 @@ def main():
                     help="run the small profiling case only (for ncu captures)")
     ap.add_argument("--profile-n", type=int, default=8192)
     ap.add_argument("--profile-dtype", default="c64")
+    ap.add_argument("--profile-ops", choices=["all", "fwd"], default="all")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.profile_case:

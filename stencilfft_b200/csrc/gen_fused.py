@@ -32,12 +32,26 @@ for dt, table in VARIANTS.items():
         for (lv, lm), vs in table.items():
             for vi, (cl, tl, nt) in enumerate(vs):
                 L.append(f"    case ({lv} << 16) | ({lm} << 8) | {vi}: "
-                         f"return launch_fused<{T[dt]}, {lv}, {lm}, {cl}, {tl}, {nt}>(prm, {'true' if inv else 'false'}, st);")
+                         f"return launch_fused<{T[dt]}, {lv}, {lm}, {cl}, {tl}, {nt}, {'true' if inv else 'false'}>(prm, st);")
         L += ["    default: break;", "    }", "    *handled = false;", "    return cudaSuccess;", "}", ""]
         if not inv:
             L += [f"int fused_variants_{dt}(int logvec, int logm) {{", "    switch ((logvec << 8) | logm) {"]
             for (lv, lm), vs in table.items():
                 L.append(f"    case ({lv} << 8) | {lm}: return {len(vs)};")
+            L += ["    default: return 0;", "    }", "}", ""]
+            # variants that can run the 2D passes on the pair-interleaved intermediate:
+            # two or more lines per tile (a pair is read and written by one tile, so the
+            # in-place y pass is race-free), two row stages (the vector side moves through
+            # registers, not 16-byte copies) and at least two columns per CTA
+            L += [f"int fused_interleave_ok_{dt}(int logvec, int logm, int variant) {{",
+                  "    switch ((logvec << 16) | (logm << 8) | variant) {"]
+            for (lv, lm), vs in table.items():
+                for vi, (cl, tl, nt) in enumerate(vs):
+                    vec, n = 1 << lv, 1 << (lv + lm)
+                    ept = tl * n // (cl * nt)
+                    ra2 = vec // min(vec, ept)
+                    if tl >= 2 and ra2 > 1 and vec // cl >= 2:
+                        L.append(f"    case ({lv} << 16) | ({lm} << 8) | {vi}: return 1;")
             L += ["    default: return 0;", "    }", "}", ""]
         L += ["}  // namespace zm", ""]
         open(f"zm_fft2_{dt}_{d}.cu", "w").write("\n".join(L))

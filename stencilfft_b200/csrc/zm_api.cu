@@ -150,6 +150,7 @@ static LineParams line_params(const zm_plan_s *p, int kind, const void *in, void
     lp.out = out;
     lp.twN = p->twN;
     lp.W = p->W;
+    lp.twd = p->twd;
     lp.twv = p->twv;
     lp.twm = p->twm;
     lp.scale_re = 1.0;
@@ -157,6 +158,16 @@ static LineParams line_params(const zm_plan_s *p, int kind, const void *in, void
     lp.apply_scale = 0;
     lp.variant = p->variant;
     lp.permute_only = (p->flags & ZM_FLAG_PERMUTE_ONLY) ? 1 : 0;
+    // 2D transforms on the size-specialised passes keep the x -> y intermediate with
+    // pairs of x-frequency rows interleaved (whole 32-byte sectors on both sides).
+    // Both passes of one transform see the same plan state, so they agree on it.
+    lp.lg_inter = 0;
+    if (p->g.dim == 2 && !lp.permute_only && p->nvariants > 0 && p->g.vp >= 2) {
+        const int ok = p->dtype == ZM_C128
+                           ? zm::fused_interleave_ok_c128(p->g.logVEC, p->g.logM, p->variant)
+                           : zm::fused_interleave_ok_c64(p->g.logVEC, p->g.logM, p->variant);
+        lp.lg_inter = ok ? 1 : 0;
+    }
     lp.nst_vec = schedule(p->g.vec, p->max_radix, lp.rad_vec);
     lp.nst_m = schedule(p->g.m, p->max_radix, lp.rad_m);
     return lp;
@@ -273,10 +284,10 @@ int zm_plan_create(zm_plan *plan, int dim, int64_t n, int64_t b, int64_t p, int 
     // precision and rounded once (FP64 for complex128; hi/lo FP32 split of the
     // FP64 value for complex64).  Replaces the L x L per-rank tables of
     // init_forward_twiddles / init_inverse_twiddles (fft.cu:37-73).
-    // Also, for the size-specialised passes: w_N^{n1 k2} in [n1][k2] order (N
-    // entries) and the sub-transform tables w_VEC^m, w_M^m.  All four tables share one
-    // allocation of 16-byte entries.
-    P->twN = P->W = P->twv = P->twm = nullptr;
+    // Also, for the size-specialised passes: w_N^m in FP64 for every dtype (the
+    // inter-step twiddles are generated from it on the device) and the sub-transform
+    // tables w_VEC^m, w_M^m.  All four tables share one allocation of 16-byte entries.
+    P->twN = P->W = P->twv = P->twm = P->twd = nullptr;
     if (flags & ZM_FLAG_HOST_ONLY) {
         *plan = P;
         return ZM_OK;
@@ -284,10 +295,10 @@ int zm_plan_create(zm_plan *plan, int dim, int64_t n, int64_t b, int64_t p, int 
     const int64_t entries = 2 * n + g.vec + g.m;
     std::vector<unsigned char> host((size_t)entries * 16);
     const long double pi = 3.141592653589793238462643383279502884L;
-    auto put = [&](int64_t slot, int64_t m, int64_t len) {   // w_len^m
+    auto put = [&](int64_t slot, int64_t m, int64_t len, bool fp64 = false) {   // w_len^m
         const long double th = -2.0L * pi * (long double)m / (long double)len;
         const double c = (double)cosl(th), s = (double)sinl(th);
-        if (dtype == ZM_C128) {
+        if (dtype == ZM_C128 || fp64) {
             double *d = reinterpret_cast<double *>(host.data()) + 2 * slot;
             d[0] = c; d[1] = s;
         } else {
@@ -298,8 +309,7 @@ int zm_plan_create(zm_plan *plan, int dim, int64_t n, int64_t b, int64_t p, int 
         }
     };
     for (int64_t m = 0; m < n; m++) put(m, m, n);
-    for (int64_t n1 = 0; n1 < g.m; n1++)
-        for (int64_t k2 = 0; k2 < g.vec; k2++) put(n + n1 * g.vec + k2, n1 * k2, n);
+    for (int64_t m = 0; m < n; m++) put(n + m, m, n, true);
     for (int64_t m = 0; m < g.vec; m++) put(2 * n + m, m, g.vec);
     for (int64_t m = 0; m < g.m; m++) put(2 * n + g.vec + m, m, g.m);
     void *tables = nullptr;
@@ -316,7 +326,7 @@ int zm_plan_create(zm_plan *plan, int dim, int64_t n, int64_t b, int64_t p, int 
     }
     unsigned char *tb = static_cast<unsigned char *>(tables);
     P->twN = tb;
-    P->W = tb + (size_t)n * 16;
+    P->twd = tb + (size_t)n * 16;
     P->twv = tb + (size_t)2 * n * 16;
     P->twm = tb + (size_t)(2 * n + g.vec) * 16;
     *plan = P;

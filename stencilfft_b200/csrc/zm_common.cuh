@@ -17,6 +17,26 @@ template <> struct __align__(8) cpx<float> { float x, y; };
 
 template <typename R> ZM_DEV cpx<R> cadd(cpx<R> a, cpx<R> b) { return {a.x + b.x, a.y + b.y}; }
 template <typename R> ZM_DEV cpx<R> csub(cpx<R> a, cpx<R> b) { return {a.x - b.x, a.y - b.y}; }
+// complex64 add / sub as one packed FP32x2 instruction each (sm_100a), same IEEE
+// round-to-nearest result per component as the scalar form
+template <> ZM_DEV cpx<float> cadd(cpx<float> a, cpx<float> b) {
+    unsigned long long A, B, D;
+    memcpy(&A, &a, 8);
+    memcpy(&B, &b, 8);
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(D) : "l"(A), "l"(B));
+    cpx<float> r;
+    memcpy(&r, &D, 8);
+    return r;
+}
+template <> ZM_DEV cpx<float> csub(cpx<float> a, cpx<float> b) {
+    unsigned long long A, B, D;
+    memcpy(&A, &a, 8);
+    memcpy(&B, &b, 8);
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(D) : "l"(A), "l"(B));
+    cpx<float> r;
+    memcpy(&r, &D, 8);
+    return r;
+}
 
 // Twiddle storage: FP64 pair for complex128, split hi/lo FP32 pairs for complex64
 // (w = hi + lo with hi = fl32(w), lo = fl32(w - hi), both from an FP64 value).
@@ -37,6 +57,18 @@ template <bool CONJ> ZM_DEV cpx<float> twmul(cpx<float> a, tw<float> w) {
     const float im_lo = fmaf(a.x, ly, a.y * w.lx);
     return {fmaf(a.x, w.x, fmaf(-a.y, wy, re_lo)), fmaf(a.x, wy, fmaf(a.y, w.x, im_lo))};
 }
+// FP64 twiddle -> stored form: itself for complex128, the hi/lo FP32 split for complex64.
+template <typename R> ZM_DEV tw<R> tw_from_d(double2 w);
+template <> ZM_DEV tw<double> tw_from_d<double>(double2 w) { return {w.x, w.y}; }
+template <> ZM_DEV tw<float> tw_from_d<float>(double2 w) {
+    const float hx = __double2float_rn(w.x), hy = __double2float_rn(w.y);
+    return {hx, hy, __double2float_rn(w.x - (double)hx), __double2float_rn(w.y - (double)hy)};
+}
+ZM_DEV double2 cmul_d(double2 a, double2 b) {
+    return {fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x)};
+}
+ZM_DEV double2 ldd2(const double2 *p) { return __ldg(p); }
+
 template <typename R> ZM_DEV tw<R> ldtw(const tw<R> *t, int64_t i) { return __ldg(t + i); }
 template <> ZM_DEV tw<double> ldtw(const tw<double> *t, int64_t i) {
     double2 v = __ldg(reinterpret_cast<const double2 *>(t) + i);

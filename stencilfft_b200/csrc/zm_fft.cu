@@ -239,13 +239,15 @@ static cudaError_t launch_typed(const LineParams &prm, int threads, size_t smem,
 int ept_for(int dtype) { return dtype == 0 ? 8 : 16; }
 
 cudaError_t launch_line_pass(const LineParams &prm, int dtype, bool inv, cudaStream_t st) {
-    if (!prm.permute_only && prm.W) {
+    if (!prm.permute_only && prm.twd) {
         bool handled = false;
         cudaError_t e;
         if (dtype == 0) e = inv ? launch_fused_c128_inv(prm, st, &handled) : launch_fused_c128_fwd(prm, st, &handled);
         else e = inv ? launch_fused_c64_inv(prm, st, &handled) : launch_fused_c64_fwd(prm, st, &handled);
         if (handled) return e;
     }
+    // the runtime-sized kernel reads and writes only the plain REPACK intermediate
+    if (prm.lg_inter != 0) return cudaErrorInvalidValue;
     const int ept = ept_for(dtype);
     const int threads = (int)((prm.T * prm.g.n) / ept);
     const size_t smem = (size_t)prm.T * prm.g.n * (dtype == 0 ? 16 : 8);

@@ -35,10 +35,12 @@ struct LineParams {
     const void *W;     // w_N^{n1 k2} in [n1][k2] order (N entries)
     const void *twv;   // w_VEC^m, m < VEC
     const void *twm;   // w_M^m, m < M
+    const void *twd;   // w_N^m, m < N, in FP64 (double2) for every dtype
     double scale_re, scale_im;
     int apply_scale;   // multiply the stored values by scale
     int variant;       // tile-shape variant of the size-specialised kernel (0 = default)
     int permute_only;  // skip all arithmetic (reference do_compute=false)
+    int lg_inter;      // 2D: log2 of the row interleave of the x -> y intermediate (0 = plain REPACK layout)
     // radix schedules of the two sub-transforms (first stage first)
     int nst_vec, nst_m;
     int rad_vec[8], rad_m[8];
@@ -57,6 +59,7 @@ struct zm_plan_s {
     void *W;          // w_N^{n1 k2}, [n1][k2] order (N entries)
     void *twv;        // w_VEC^m (VEC entries)
     void *twm;        // w_M^m (M entries)
+    void *twd;        // w_N^m in FP64 (N entries; the same table as twN for complex128)
     int T[3];         // lines per CTA for the passes (x, y, z)
     int max_radix;
     int variant;      // tile-shape variant of the size-specialised kernel
