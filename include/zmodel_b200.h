@@ -101,6 +101,17 @@ int zm_plan_workspace_size(zm_plan plan, size_t *bytes);
  */
 int zm_plan_kernel_variants(zm_plan plan, int *count);
 int zm_plan_set_kernel_variant(zm_plan plan, int variant);
+/*
+ * Autotuner (no counterpart in the reference, whose only tuning knob is the
+ * compile-time B_DIM): times a forward + inverse round trip `reps` times per kernel
+ * variant on `stream` (CUDA events, after one untimed round trip), makes the fastest
+ * the plan's variant and returns it with its time per round trip in milliseconds
+ * (either output may be NULL).  `a`, `b` and `work` are caller fields of the plan's
+ * size; their contents are overwritten (a holds IFFT(FFT(a)) / n^dim at the end, equal
+ * to the input up to rounding).  Synchronises `stream`; not capturable.
+ */
+int zm_plan_autotune(zm_plan plan, void *a, void *b, void *work, int reps, void *stream,
+                     int *best_variant, float *best_ms);
 
 /*
  * Transforms over all virtual ranks.

@@ -58,6 +58,8 @@ SIGNATURES = {
     "zm_plan_workspace_size": [_P, ctypes.POINTER(ctypes.c_size_t)],
     "zm_plan_kernel_variants": [_P, ctypes.POINTER(ctypes.c_int)],
     "zm_plan_set_kernel_variant": [_P, ctypes.c_int],
+    "zm_plan_autotune": [_P, _P, _P, _P, ctypes.c_int, _P, ctypes.POINTER(ctypes.c_int),
+                         ctypes.POINTER(ctypes.c_float)],
     "zm_fft_forward": [_P, _P, _P, _P, _P],
     "zm_fft_inverse": [_P, _P, _P, _P, _D, _D, _P],
     "zm_fft_inverse_static": [_P, _P, _P, _D, _D, _P],

@@ -1,6 +1,8 @@
 """Generates zm_fft2_<dtype>_<dir>.cu: the size-specialised fused passes and their
 dispatch tables.  Each (log2 VEC, log2 M) pair lists variants (cluster size CL, lines
-per tile TL, threads NT); the plan's `variant` picks one (0 = default)."""
+per tile TL, threads NT); the plan's `variant` picks one.  Variant 0, the default, is
+the fastest one measured on B200 at the sizes the table was tuned on; zm_plan_autotune
+re-measures them for a plan."""
 VARIANTS = {
     "c64": {
         (4, 4): [(1, 32, 512)], (4, 5): [(1, 16, 512)], (4, 6): [(1, 8, 512), (1, 4, 256)],
@@ -9,13 +11,13 @@ VARIANTS = {
         (4, 8): [(1, 2, 512), (2, 4, 512)],
         (5, 8): [(2, 2, 512), (1, 1, 512), (2, 1, 256)],
         (6, 7): [(1, 1, 512), (2, 2, 512)],
-        (6, 8): [(2, 1, 512), (4, 2, 512), (1, 1, 1024)],
+        (6, 8): [(4, 2, 512), (2, 1, 512), (1, 1, 1024)],
     },
     "c128": {
         (4, 4): [(1, 16, 256)], (4, 5): [(1, 8, 256)], (4, 6): [(1, 4, 256)], (2, 7): [(1, 8, 256)],
         (5, 6): [(1, 2, 256)], (5, 7): [(1, 1, 256), (2, 2, 256)], (4, 8): [(1, 1, 256), (2, 2, 256)],
-        (5, 8): [(2, 1, 256), (1, 1, 512)], (6, 7): [(2, 1, 256), (1, 1, 512)],
-        (6, 8): [(4, 1, 256), (2, 1, 512), (4, 2, 512)],
+        (5, 8): [(1, 1, 512), (2, 1, 256)], (6, 7): [(2, 1, 256), (1, 1, 512)],
+        (6, 8): [(2, 1, 512), (4, 1, 256), (4, 2, 512)],
     },
 }
 T = {"c64": "float", "c128": "double"}

@@ -358,6 +358,60 @@ int zm_plan_set_kernel_variant(zm_plan plan, int variant) {
     return ZM_OK;
 }
 
+int zm_plan_autotune(zm_plan plan, void *a, void *b, void *work, int reps, void *stream,
+                     int *best_variant, float *best_ms) {
+    int rc;
+    if ((rc = check_device_plan(plan))) return rc;
+    if (reps < 1) return fail(ZM_ERR_INVALID_ARG, "reps must be >= 1 (got %d)", reps);
+    if ((rc = check_field(plan, a, "a")) || (rc = check_field(plan, b, "b"))) return rc;
+    if (work && (rc = check_field(plan, work, "work"))) return rc;
+    const int nv = plan->nvariants > 0 ? plan->nvariants : 1;
+    double inv_n = 1.0;
+    for (int d = 0; d < plan->g.dim; d++) inv_n /= (double)plan->g.n;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t ce = cudaEventCreate(&e0);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+    if (ce != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        return cuda_fail(ce, "autotune events");
+    }
+    const int saved = plan->variant;
+    int best = 0;
+    float best_t = 0.f;
+    rc = ZM_OK;
+    for (int v = 0; v < nv && rc == ZM_OK; v++) {
+        plan->variant = v;
+        for (int it = -1; it < reps && rc == ZM_OK; it++) {
+            if (it == 0) cudaEventRecord(e0, (cudaStream_t)stream);
+            rc = zm_fft_forward(plan, a, b, work, stream);
+            if (rc == ZM_OK) rc = zm_fft_inverse(plan, b, a, work, inv_n, 0.0, stream);
+        }
+        if (rc != ZM_OK) break;
+        cudaEventRecord(e1, (cudaStream_t)stream);
+        if ((ce = cudaEventSynchronize(e1)) != cudaSuccess) {
+            rc = cuda_fail(ce, "autotune timing");
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= (float)reps;
+        if (v == 0 || ms < best_t) {
+            best = v;
+            best_t = ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != ZM_OK) {
+        plan->variant = saved;
+        return rc;
+    }
+    plan->variant = best;
+    if (best_variant) *best_variant = best;
+    if (best_ms) *best_ms = best_t;
+    return ZM_OK;
+}
+
 int zm_plan_workspace_size(zm_plan plan, size_t *bytes) {
     int rc;
     if ((rc = check_plan(plan))) return rc;

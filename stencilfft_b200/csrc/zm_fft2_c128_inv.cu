@@ -18,12 +18,12 @@ cudaError_t launch_fused_c128_inv(const LineParams &prm, cudaStream_t st, bool *
     case (5 << 16) | (7 << 8) | 1: return launch_fused<double, 5, 7, 2, 2, 256, true>(prm, st);
     case (4 << 16) | (8 << 8) | 0: return launch_fused<double, 4, 8, 1, 1, 256, true>(prm, st);
     case (4 << 16) | (8 << 8) | 1: return launch_fused<double, 4, 8, 2, 2, 256, true>(prm, st);
-    case (5 << 16) | (8 << 8) | 0: return launch_fused<double, 5, 8, 2, 1, 256, true>(prm, st);
-    case (5 << 16) | (8 << 8) | 1: return launch_fused<double, 5, 8, 1, 1, 512, true>(prm, st);
+    case (5 << 16) | (8 << 8) | 0: return launch_fused<double, 5, 8, 1, 1, 512, true>(prm, st);
+    case (5 << 16) | (8 << 8) | 1: return launch_fused<double, 5, 8, 2, 1, 256, true>(prm, st);
     case (6 << 16) | (7 << 8) | 0: return launch_fused<double, 6, 7, 2, 1, 256, true>(prm, st);
     case (6 << 16) | (7 << 8) | 1: return launch_fused<double, 6, 7, 1, 1, 512, true>(prm, st);
-    case (6 << 16) | (8 << 8) | 0: return launch_fused<double, 6, 8, 4, 1, 256, true>(prm, st);
-    case (6 << 16) | (8 << 8) | 1: return launch_fused<double, 6, 8, 2, 1, 512, true>(prm, st);
+    case (6 << 16) | (8 << 8) | 0: return launch_fused<double, 6, 8, 2, 1, 512, true>(prm, st);
+    case (6 << 16) | (8 << 8) | 1: return launch_fused<double, 6, 8, 4, 1, 256, true>(prm, st);
     case (6 << 16) | (8 << 8) | 2: return launch_fused<double, 6, 8, 4, 2, 512, true>(prm, st);
     default: break;
     }

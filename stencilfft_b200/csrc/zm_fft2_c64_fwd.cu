@@ -25,8 +25,8 @@ cudaError_t launch_fused_c64_fwd(const LineParams &prm, cudaStream_t st, bool *h
     case (5 << 16) | (8 << 8) | 2: return launch_fused<float, 5, 8, 2, 1, 256, false>(prm, st);
     case (6 << 16) | (7 << 8) | 0: return launch_fused<float, 6, 7, 1, 1, 512, false>(prm, st);
     case (6 << 16) | (7 << 8) | 1: return launch_fused<float, 6, 7, 2, 2, 512, false>(prm, st);
-    case (6 << 16) | (8 << 8) | 0: return launch_fused<float, 6, 8, 2, 1, 512, false>(prm, st);
-    case (6 << 16) | (8 << 8) | 1: return launch_fused<float, 6, 8, 4, 2, 512, false>(prm, st);
+    case (6 << 16) | (8 << 8) | 0: return launch_fused<float, 6, 8, 4, 2, 512, false>(prm, st);
+    case (6 << 16) | (8 << 8) | 1: return launch_fused<float, 6, 8, 2, 1, 512, false>(prm, st);
     case (6 << 16) | (8 << 8) | 2: return launch_fused<float, 6, 8, 1, 1, 1024, false>(prm, st);
     default: break;
     }
@@ -58,7 +58,7 @@ int fused_interleave_ok_c64(int logvec, int logm, int variant) {
     case (5 << 16) | (7 << 8) | 2: return 1;
     case (5 << 16) | (8 << 8) | 0: return 1;
     case (6 << 16) | (7 << 8) | 1: return 1;
-    case (6 << 16) | (8 << 8) | 1: return 1;
+    case (6 << 16) | (8 << 8) | 0: return 1;
     default: return 0;
     }
 }

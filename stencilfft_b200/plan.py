@@ -106,6 +106,16 @@ class Plan:
     def set_kernel_variant(self, variant: int) -> None:
         check(lib().zm_plan_set_kernel_variant(self._h, int(variant)), "zm_plan_set_kernel_variant")
 
+    def autotune(self, a, b, work=None, reps: int = 3, stream=None) -> tuple[int, float]:
+        """Time a forward + inverse round trip per kernel variant and keep the fastest.
+
+        `a`, `b`, `work` are overwritten; returns (variant, ms per round trip)."""
+        self._check(a, "a"), self._check(b, "b")
+        v, ms = ctypes.c_int(), ctypes.c_float()
+        check(lib().zm_plan_autotune(self._h, _ptr(a), _ptr(b), _ptr(work), int(reps), _stream_ptr(stream),
+                                     ctypes.byref(v), ctypes.byref(ms)), "zm_plan_autotune")
+        return v.value, ms.value
+
     # ------------------------------------------------------------ transforms
     def forward_fft(self, buf0, buf1, work=None, stream=None):
         """forward_fft / forward_fft_3d: real layout buf0 -> reciprocal layout buf1."""

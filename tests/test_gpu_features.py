@@ -167,3 +167,24 @@ def test_launch_counter_advances():
     pl.forward_fft(d, o)
     pl.laplace(d, o)
     assert launch_count() - before == 3
+
+
+@pytest.mark.parametrize("dt", ["c64", "c128"])
+def test_autotune_keeps_results(dt):
+    """zm_plan_autotune: picks a listed variant, leaves a = IFFT(FFT(a)) / N^2, and the
+    tuned plan still matches the oracle."""
+    import torch
+    n, b, p = 4096, 32, 4
+    pl = _plan(2, n, b, p, dt)
+    assert pl.kernel_variants >= 2
+    x = O.natural_to_real_layout(rand_field(2, n, 7), b, p)
+    a = to_dev(x, dt)
+    bb, w = torch.empty_like(a), torch.empty_like(a)
+    v, ms = pl.autotune(a, bb, work=w, reps=2)
+    assert 0 <= v < pl.kernel_variants and ms > 0
+    # a went through (reps + 1) round trips per variant: rounding accumulates in c64
+    tol = 1e-12 if dt == "c128" else 5e-6
+    assert relerr(to_host(a), x) < tol
+    a = to_dev(x, dt)
+    pl.forward_fft(a, bb, work=w)
+    assert relerr(to_host(bb), O.forward_fft(x, 2, n, b, p)) < TOL[dt]
