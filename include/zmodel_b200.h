@@ -221,6 +221,9 @@ int zm_reciprocal_to_natural(zm_plan plan, const void *interleaved, void *natura
  */
 enum zm_spectral_op { ZM_SPECTRAL_GAUSSIAN = 0, ZM_SPECTRAL_POISSON = 1, ZM_SPECTRAL_SCALE = 2 };
 int zm_spectral_apply(zm_plan plan, void *data, int op, double a, void *stream);
+/* VJP of zm_spectral_apply, in place on `grad` (no reference counterpart).  The
+ * multipliers are real and diagonal, so the adjoint applies the same multiplier. */
+int zm_spectral_apply_vjp(zm_plan plan, void *grad, int op, double a, void *stream);
 
 /*
  * Seeded synthetic fields written straight into the real-space layout

@@ -270,10 +270,6 @@ def ref_host_lib(n: int, b: int, p: int):
     return L
 
 
-def ref_gpu_lib_path(n: int, b: int, p: int) -> Path:
-    return REF_DIR / f"libzref_gpu_N{n}_B{b}_P{p}.so"
-
-
 def ref_available() -> bool:
     return REF_DIR.exists() and any(REF_DIR.glob("libzref_host_*.so"))
 

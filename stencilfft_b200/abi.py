@@ -78,6 +78,7 @@ SIGNATURES = {
     "zm_natural_to_reciprocal": [_P, _P, _P, _P],
     "zm_reciprocal_to_natural": [_P, _P, _P, _P],
     "zm_spectral_apply": [_P, _P, ctypes.c_int, _D, _P],
+    "zm_spectral_apply_vjp": [_P, _P, ctypes.c_int, _D, _P],
     "zm_fill_field": [_P, _P, ctypes.c_int, ctypes.c_uint64, _P],
     "zm_fill_modes": [_P, _P, ctypes.c_int, _PI64, ctypes.POINTER(_D), _D, ctypes.c_uint64, _P],
     "zm_real_to_global": [_P, _i64, _i64, _i64, _i64, _i64, _i64, _PI64, _PI64, _PI64],

@@ -533,6 +533,11 @@ int zm_spectral_apply(zm_plan plan, void *data, int op, double a, void *stream) 
     return ZM_OK;
 }
 
+int zm_spectral_apply_vjp(zm_plan plan, void *grad, int op, double a, void *stream) {
+    // every operator is a real diagonal multiplier, hence self-adjoint
+    return zm_spectral_apply(plan, grad, op, a, stream);
+}
+
 int zm_fill_field(zm_plan plan, void *interleaved, int kind, uint64_t seed, void *stream) {
     int rc;
     if ((rc = check_device_plan(plan))) return rc;

@@ -217,6 +217,13 @@ class Plan:
               "zm_spectral_apply")
         return data
 
+    def spectral_apply_vjp(self, grad, op: int, a: float, stream=None):
+        """VJP of spectral_apply (in place; the real diagonal multipliers are self-adjoint)."""
+        self._check(grad, "grad")
+        check(lib().zm_spectral_apply_vjp(self._h, _ptr(grad), int(op), float(a), _stream_ptr(stream)),
+              "zm_spectral_apply_vjp")
+        return grad
+
     def fill(self, out, kind: int, seed: int, stream=None):
         self._check(out, "out")
         check(lib().zm_fill_field(self._h, _ptr(out), int(kind), int(seed), _stream_ptr(stream)),
