@@ -249,6 +249,60 @@ int zm_reciprocal_to_global(zm_plan plan, int64_t rid, int64_t cid, int64_t did,
 int zm_global_to_reciprocal(zm_plan plan, int64_t kd, int64_t kr, int64_t kc, int64_t *rid,
                             int64_t *cid, int64_t *did, int64_t *ld, int64_t *lr, int64_t *lc);
 
+/*
+ * Batches of independent 2D fields of uneven N (no reference counterpart: the reference
+ * transforms one field per MPI job).  Every field has its own (N, B, P) and lives in the
+ * reference layout of that plan at `offset` elements into a batch buffer (offsets are
+ * multiples of 2 elements, so a 16-byte aligned buffer keeps every field aligned).  Each
+ * call below is ONE cooperative persistent launch over all fields (grid = the resident
+ * CTAs of the device, phases separated by a grid barrier whose waits are bounded); no
+ * call allocates or synchronises, so a sequence of calls can be captured in a CUDA graph.
+ * Fields need 64 <= N <= 4096 (complex64) or 32 <= N <= 2048 (complex128).  A grid
+ * barrier that waits more than 2 s sets a device error flag instead of hanging:
+ * zm_batch_status reads and clears it.
+ */
+typedef struct zm_batch_s *zm_batch;
+typedef struct {
+    int64_t n, b, p;
+    int64_t offset;   /* element offset of the field in a batch buffer */
+    int64_t elems;    /* N * N */
+} zm_batch_field;
+int zm_batch_create(zm_batch *batch, int nfields, const int64_t *n, const int64_t *b,
+                    const int64_t *p, int dtype);
+int zm_batch_destroy(zm_batch batch);
+int zm_batch_get_field(zm_batch batch, int i, zm_batch_field *info);
+/* Elements of one batch buffer (sum of N^2 plus alignment padding). */
+int zm_batch_total_elems(zm_batch batch, int64_t *elems);
+/* Field i <- zm_fill_field(kind, first_seed + i) in its real layout. */
+int zm_batch_fill(zm_batch batch, void *data, int kind, uint64_t first_seed, void *stream);
+/* Per field: zm_fft_forward (in kept) / zm_fft_inverse with scale 1 / N^2 when
+ * `normalise` is non-zero (work NULL: `in` is scratch). */
+int zm_batch_forward(zm_batch batch, const void *in, void *out, void *stream);
+int zm_batch_inverse(zm_batch batch, const void *in, void *out, void *work, int normalise,
+                     void *stream);
+/*
+ * Spectral Poisson solve per field on a periodic square of side `length` (h = length / N):
+ * phi = IFFT(FFT(rhs) / (-|k|^2)) with k = (2 pi / length) * (signed integer frequency),
+ * the k = 0 mode set to 0, then (when `residual` is not NULL)
+ * residual = Lap_h(phi) - rhs with the 5-point Laplacian / h^2.  The forward y pass, the
+ * division and the inverse y pass are fused (the spectrum is never stored).  `work` holds
+ * one batch buffer of scratch; rhs is kept.
+ */
+int zm_batch_poisson(zm_batch batch, const void *rhs, void *phi, void *residual, void *work,
+                     double length, void *stream);
+/* Synchronises the device and reports (then clears) the grid-barrier timeout flag:
+ * *device_error = 1 when a barrier timed out since the last call. */
+int zm_batch_status(zm_batch batch, int *device_error);
+/*
+ * B autotuner for batched fields (the reference's compile-time B_DIM knob): times
+ * zm_batch_poisson on a batch of `count` fields of size N for every B allowed by the
+ * layout constraints (power of two, B | N/P, P | N/(P B)), `reps` timed calls each after
+ * one untimed call, and returns the fastest B and its time per call.  Allocates and frees
+ * its own buffers and synchronises the device.
+ */
+int zm_batch_autotune_b(int64_t n, int64_t p, int dtype, int count, int reps, int64_t *best_b,
+                        float *best_ms);
+
 /* Diagnostics. */
 const char *zm_last_error_string(void);
 const char *zm_status_string(int status);

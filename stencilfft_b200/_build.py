@@ -21,7 +21,7 @@ OUT_DIR = PKG / "lib"
 LIB = OUT_DIR / "libzmodel_b200.so"
 BUILD_DIR = ROOT / "_build" / "zmodel_b200"
 
-SOURCES = ["zm_api.cu", "zm_fft.cu", "zm_stencil.cu", "zm_layout.cu", "zm_static.cu", "zm_fft2_c64_fwd.cu",
+SOURCES = ["zm_api.cu", "zm_fft.cu", "zm_stencil.cu", "zm_layout.cu", "zm_static.cu", "zm_batch.cu", "zm_fft2_c64_fwd.cu",
            "zm_fft2_c64_inv.cu", "zm_fft2_c128_fwd.cu", "zm_fft2_c128_inv.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",

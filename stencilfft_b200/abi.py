@@ -44,6 +44,10 @@ class zm_plan_info(ctypes.Structure):
                 ("workspace_bytes", ctypes.c_size_t)]
 
 
+class zm_batch_field(ctypes.Structure):
+    _fields_ = [("n", _i64), ("b", _i64), ("p", _i64), ("offset", _i64), ("elems", _i64)]
+
+
 class ZmError(RuntimeError):
     def __init__(self, status: int, what: str, detail: str):
         super().__init__(f"{what} failed with status {status}: {detail}")
@@ -85,6 +89,17 @@ SIGNATURES = {
     "zm_global_to_real": [_P, _i64, _i64, _i64, _PI64, _PI64, _PI64, _PI64, _PI64, _PI64],
     "zm_reciprocal_to_global": [_P, _i64, _i64, _i64, _i64, _i64, _i64, _PI64, _PI64, _PI64],
     "zm_global_to_reciprocal": [_P, _i64, _i64, _i64, _PI64, _PI64, _PI64, _PI64, _PI64, _PI64],
+    "zm_batch_create": [ctypes.POINTER(_P), ctypes.c_int, _PI64, _PI64, _PI64, ctypes.c_int],
+    "zm_batch_destroy": [_P],
+    "zm_batch_get_field": [_P, ctypes.c_int, ctypes.POINTER(zm_batch_field)],
+    "zm_batch_total_elems": [_P, _PI64],
+    "zm_batch_fill": [_P, _P, ctypes.c_int, ctypes.c_uint64, _P],
+    "zm_batch_forward": [_P, _P, _P, _P],
+    "zm_batch_inverse": [_P, _P, _P, _P, ctypes.c_int, _P],
+    "zm_batch_poisson": [_P, _P, _P, _P, _P, _D, _P],
+    "zm_batch_status": [_P, ctypes.POINTER(ctypes.c_int)],
+    "zm_batch_autotune_b": [_i64, _i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, _PI64,
+                            ctypes.POINTER(ctypes.c_float)],
     "zm_last_error_string": [],
     "zm_status_string": [ctypes.c_int],
     "zm_launch_count": [],

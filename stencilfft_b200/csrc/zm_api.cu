@@ -41,9 +41,17 @@ int ilog2(int64_t x) {
 
 bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+int schedule(int64_t n, int rmax, int *rad) { return zm::radix_schedule(n, rmax, rad); }
+
+}  // namespace
+
+namespace zm {
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
 // Radix schedule of a power-of-two length n with radices <= rmax: the
 // remainder radix first, then rmax-radix stages.
-int schedule(int64_t n, int rmax, int *rad) {
+int radix_schedule(int64_t n, int rmax, int *rad) {
     int ln = ilog2(n), lr = ilog2(rmax), k = 0;
     if (ln == 0) return 0;
     int rem = ln % lr;
@@ -51,12 +59,6 @@ int schedule(int64_t n, int rmax, int *rad) {
     for (int i = 0; i < ln / lr; i++) rad[k++] = rmax;
     return k;
 }
-
-}  // namespace
-
-namespace zm {
-
-void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 int report_error(int code, const char *fmt, ...) {
     char buf[512];

@@ -1,0 +1,574 @@
+// zm_batch.cu -- many independent 2D fields of uneven N in one persistent launch.
+//
+// A batch is a list of fields, each with its own (N, B, P) reference layout, packed one
+// after the other in every batch buffer.  One call is one cooperative launch of
+// batch_kernel: a grid of exactly the CTAs that fit on the device at once walks a short
+// program of steps (an axis pass over all fields, a fused y pass, a stencil, a
+// generator ...), with a grid barrier between steps.  Inside a pass step the work items
+// are tiles of TL lines of one field, TL * N = a fixed number of points per tile, so the
+// same CTA shape serves every N; a tile's field comes from a binary search over the
+// fields' first tile numbers.  The tile code is the runtime-sized axis pass of
+// zm_tile.cuh (the same Cooley-Tukey split and reference layouts as single-field plans).
+#include <cuda/atomic>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <new>
+#include <tuple>
+#include <vector>
+
+#include "zm_index.cuh"
+#include "zm_internal.h"
+#include "zm_tile.cuh"
+#include "zmodel_b200.h"
+
+namespace zm {
+
+constexpr int kBatchThreads = 256;
+constexpr int kMaxSteps = 6;
+constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;   // 2 s
+
+struct BatchField {
+    Geom g;
+    int64_t off;       // element offset in a batch buffer
+    int64_t tile0;     // first tile of this field in a pass step's tile sequence
+    const void *twN;   // the field plan's twiddle table w_N^m (tw<T> entries)
+    int T;             // lines per tile
+    int nst_vec, nst_m;
+    int rad_vec[8], rad_m[8];
+};
+
+enum BatchOp : int {
+    BOP_X_FWD = 0,     // x pass forward: real layout -> REPACK layout
+    BOP_Y_FWD = 1,     // y pass forward: REPACK layout -> reciprocal layout
+    BOP_Y_INV = 2,     // y pass inverse
+    BOP_X_INV = 3,     // x pass inverse (scale 1/N^2 when step.scale)
+    BOP_Y_POISSON = 4, // y pass forward, divide by -|k|^2, y pass inverse (in place)
+    BOP_RESIDUAL = 5,  // out = Lap(in) / h^2 - aux (5-point, periodic)
+    BOP_FILL = 6       // out = generator(kind, seed + field) in the real layout
+};
+
+struct BatchStep {
+    int op;
+    int kind;          // BOP_FILL: zm_field_kind
+    int scale;         // BOP_X_INV: apply 1/N^2
+    const void *in;
+    void *out;
+    const void *aux;
+    double a;          // BOP_Y_POISSON: 2 pi / length; BOP_RESIDUAL: 1 / length
+    uint64_t seed;
+};
+
+struct BatchParams {
+    const BatchField *fields;
+    int nfields;
+    int64_t tiles;
+    int nsteps;
+    BatchStep step[kMaxSteps];
+    unsigned *bar;     // [0] arrivals, [1] generation
+    int *err;          // set to 1 by a barrier that timed out
+};
+
+ZM_DEV unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid-wide barrier of a cooperative launch (all CTAs resident).  Sense by generation
+// count; the last CTA to arrive resets the arrival count and releases the generation.
+// A wait longer than kBarrierTimeoutNs, or a flag already raised by another CTA, makes
+// every waiting CTA give up: returns false and the kernel returns.
+ZM_DEV bool grid_barrier(unsigned *bar, unsigned nblocks, int *err, int *s_ok) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(bar[0]), gen(bar[1]);
+        cuda::atomic_ref<int, cuda::thread_scope_device> flag(*err);
+        const unsigned g0 = gen.load(cuda::memory_order_acquire);
+        if (cnt.fetch_add(1u, cuda::memory_order_acq_rel) == nblocks - 1) {
+            cnt.store(0u, cuda::memory_order_relaxed);
+            gen.fetch_add(1u, cuda::memory_order_release);
+        } else {
+            const unsigned long long t0 = globaltimer_ns();
+            while (gen.load(cuda::memory_order_acquire) == g0) {
+                if (flag.load(cuda::memory_order_relaxed) != 0 ||
+                    globaltimer_ns() - t0 > kBarrierTimeoutNs) {
+                    flag.store(1, cuda::memory_order_relaxed);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(128);
+            }
+        }
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+// largest f with fields[f].tile0 <= tile
+ZM_DEV int field_of_tile(const BatchField *fields, int nfields, int64_t tile) {
+    int lo = 0, hi = nfields - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (fields[mid].tile0 <= tile) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// signed frequency
+ZM_DEV double sfreq(int64_t k, const Geom &g) { return (double)(k >= (g.n >> 1) ? k - g.n : k); }
+
+// global (row, col) -> element of the real layout (inverse of real_gidx, 2D)
+ZM_DEV int64_t real_elem(int64_t gr, int64_t gc, const Geom &g) {
+    const int64_t rid = (gr >> g.logB) & (g.p - 1);
+    const int64_t lr = ((gr >> (g.logB + g.logP)) << g.logB) + (gr & (g.b - 1));
+    const int64_t cid = (gc >> g.logB) & (g.p - 1);
+    const int64_t pos = ((gc & (g.b - 1)) << g.logVEC) + (gc >> (g.logB + g.logP));
+    return (((rid << g.logP) + cid) << (2 * g.logL)) + (lr << g.logL) + pos;
+}
+
+template <typename T, int EPT>
+__global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(const BatchParams bp) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<T> *s = reinterpret_cast<cpx<T> *>(smem_raw);
+    __shared__ int64_t s_abase[64], s_fbase[64];
+    __shared__ BatchField sf;
+    __shared__ int s_ok;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+
+    for (int st = 0; st < bp.nsteps; st++) {
+        if (st > 0 && !grid_barrier(bp.bar, gridDim.x, bp.err, &s_ok)) return;
+        const BatchStep S = bp.step[st];
+
+        if (S.op == BOP_RESIDUAL || S.op == BOP_FILL) {
+            // element-wise steps: field by field, grid-stride inside each field
+            const int64_t stride = (int64_t)gridDim.x * nthr;
+            for (int f = 0; f < bp.nfields; f++) {
+                const BatchField &F = bp.fields[f];
+                const Geom g = F.g;
+                const int64_t total = g.n * g.n;
+                cpx<T> *out = reinterpret_cast<cpx<T> *>(S.out) + F.off;
+                if (S.op == BOP_FILL) {
+                    const uint64_t seed = S.seed + (uint64_t)f;
+                    for (int64_t e = (int64_t)blockIdx.x * nthr + tid; e < total; e += stride) {
+                        const uint64_t gi = (uint64_t)real_gidx(e, g);
+                        double re, im;
+                        if (S.kind == 0) {
+                            re = u01(seed, gi, 0) * 2.0 - 1.0;
+                            im = u01(seed, gi, 1) * 2.0 - 1.0;
+                        } else {
+                            re = gauss(seed, gi, 0);
+                            im = gauss(seed, gi, 1);
+                        }
+                        out[e] = {(T)re, (T)im};
+                    }
+                } else {
+                    const cpx<T> *in = reinterpret_cast<const cpx<T> *>(S.in) + F.off;
+                    const cpx<T> *rhs = reinterpret_cast<const cpx<T> *>(S.aux) + F.off;
+                    const T inv_h2 = (T)((double)g.n * S.a * (double)g.n * S.a);
+                    for (int64_t e = (int64_t)blockIdx.x * nthr + tid; e < total; e += stride) {
+                        const int64_t gi = real_gidx(e, g);
+                        const int64_t gr = gi >> g.logN, gc = gi & (g.n - 1);
+                        const int64_t m = g.n - 1;
+                        const cpx<T> up = ldg(in + real_elem((gr - 1) & m, gc, g));
+                        const cpx<T> dn = ldg(in + real_elem((gr + 1) & m, gc, g));
+                        const cpx<T> lf = ldg(in + real_elem(gr, (gc - 1) & m, g));
+                        const cpx<T> rt = ldg(in + real_elem(gr, (gc + 1) & m, g));
+                        const cpx<T> c = ldg(in + e), r = ldg(rhs + e);
+                        const T lx = up.x + dn.x + lf.x + rt.x - (T)4 * c.x;
+                        const T ly = up.y + dn.y + lf.y + rt.y - (T)4 * c.y;
+                        out[e] = {lx * inv_h2 - r.x, ly * inv_h2 - r.y};
+                    }
+                }
+            }
+            continue;
+        }
+
+        // axis-pass steps: tiles of TL lines, TL * N = nthr * EPT points
+        for (int64_t tile = blockIdx.x; tile < bp.tiles; tile += gridDim.x) {
+            __syncthreads();   // the previous tile is done with sf, the bases and s
+            if (tid == 0) sf = bp.fields[field_of_tile(bp.fields, bp.nfields, tile)];
+            __syncthreads();
+            const Geom &g = sf.g;
+            const int64_t l0 = (tile - sf.tile0) * sf.T;
+            const bool xpass = S.op == BOP_X_FWD || S.op == BOP_X_INV;
+            const Tile c = tile_begin(g, xpass ? PASS_X2 : PASS_Y2, l0, sf.T, s_abase, s_fbase, nthr, tid);
+            __syncthreads();
+            const cpx<T> *in = reinterpret_cast<const cpx<T> *>(S.in) + sf.off;
+            cpx<T> *out = reinterpret_cast<cpx<T> *>(S.out) + sf.off;
+            const tw<T> *twN = reinterpret_cast<const tw<T> *>(sf.twN);
+            if (S.op == BOP_X_FWD || S.op == BOP_Y_FWD) {
+                tile_load_vec(c, g, s, in, nthr, tid);
+                __syncthreads();
+                tile_transform<T, EPT, false>(s, g, sf.rad_vec, sf.nst_vec, sf.rad_m, sf.nst_m, nthr, tid, twN);
+                tile_store_freq(c, g, s, out, false, (T)1, (T)0, nthr, tid);
+            } else if (S.op == BOP_X_INV || S.op == BOP_Y_INV) {
+                tile_load_freq(c, g, s, in, nthr, tid);
+                __syncthreads();
+                tile_transform<T, EPT, true>(s, g, sf.rad_vec, sf.nst_vec, sf.rad_m, sf.nst_m, nthr, tid, twN);
+                const bool scl = S.scale && xpass;
+                const T sc = (T)(1.0 / ((double)g.n * (double)g.n));
+                tile_store_vec(c, g, s, out, scl, sc, (T)0, nthr, tid);
+            } else {   // BOP_Y_POISSON
+                tile_load_vec(c, g, s, in, nthr, tid);
+                __syncthreads();
+                tile_transform<T, EPT, false>(s, g, sf.rad_vec, sf.nst_vec, sf.rad_m, sf.nst_m, nthr, tid, twN);
+                // slot (t, k1, k2) holds the frequency the y pass would store at rank
+                // (rid = k2 / VP, cid), local row p, column pos = k1 VP + k2 % VP
+                // (reciprocal_to_global, utils.h:265-268)
+                const int tot = sf.T << g.logN;
+                const double a2 = S.a * S.a;
+                for (int e = tid; e < tot; e += nthr) {
+                    const int t = e >> g.logN, r = e & (int)(g.n - 1);
+                    const int k1 = r >> g.logVEC, k2 = r & (int)(g.vec - 1);
+                    const int64_t rid = k2 >> g.logVP;
+                    const int64_t pos = ((int64_t)k1 << g.logVP) + (k2 & (int)(g.vp - 1));
+                    const int64_t l = l0 + t, cid = l >> g.logL, p = l & (g.L - 1);
+                    const double sa = sfreq(d_ct(cid * g.L + d_lp(p, g), g), g);
+                    const double sb = sfreq(d_ct(rid * g.L + d_lp(pos, g), g), g);
+                    const double ksq = sa * sa + sb * sb;
+                    const double fac = ksq == 0.0 ? 0.0 : -1.0 / (a2 * ksq);
+                    const cpx<T> v = s[e];
+                    s[e] = {(T)(v.x * fac), (T)(v.y * fac)};
+                }
+                __syncthreads();
+                tile_transform<T, EPT, true>(s, g, sf.rad_vec, sf.nst_vec, sf.rad_m, sf.nst_m, nthr, tid, twN);
+                tile_store_vec(c, g, s, out, false, (T)1, (T)0, nthr, tid);
+            }
+        }
+    }
+}
+
+template <typename T, int EPT>
+static cudaError_t launch_batch_t(const BatchParams &bp, int grid, cudaStream_t st) {
+    const size_t smem = sizeof(cpx<T>) * kBatchThreads * EPT;
+    cudaError_t e = cudaMemsetAsync(bp.bar, 0, 2 * sizeof(unsigned), st);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kBatchThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, batch_kernel<T, EPT>, bp);
+    count_launch();
+    return e;
+}
+
+template <typename T, int EPT>
+static int batch_grid_t(int device) {
+    int per_sm = 0, sms = 0;
+    const size_t smem = sizeof(cpx<T>) * kBatchThreads * EPT;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<T, EPT>, kBatchThreads, smem) !=
+        cudaSuccess)
+        return 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+    return per_sm * sms;
+}
+
+}  // namespace zm
+
+// ================================================================== C ABI
+
+struct zm_batch_s {
+    int dtype;
+    int device;
+    int grid;
+    std::vector<zm_plan> plans;            // distinct (N, B, P) plans (twiddle tables)
+    std::vector<zm::BatchField> fields;    // host copy
+    std::vector<int> field_plan;
+    zm::BatchField *d_fields = nullptr;
+    unsigned *d_sync = nullptr;            // [0..1] barrier, [2] error flag
+    int64_t tiles = 0, elems = 0;
+};
+
+namespace {
+
+bool aligned16b(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+int check_batch(zm_batch b) {
+    if (!b) return zm::report_error(ZM_ERR_INVALID_ARG, "null batch");
+    return ZM_OK;
+}
+
+int check_buf(const void *p, const char *name) {
+    if (!p) return zm::report_error(ZM_ERR_INVALID_ARG, "%s is NULL", name);
+    if (!aligned16b(p)) return zm::report_error(ZM_ERR_MISALIGNED, "%s is not 16-byte aligned", name);
+    return ZM_OK;
+}
+
+bool overlap_b(const void *a, const void *b, size_t bytes) {
+    const char *x = static_cast<const char *>(a), *y = static_cast<const char *>(b);
+    return x < y + bytes && y < x + bytes;
+}
+
+int launch(zm_batch b, const zm::BatchStep *steps, int nsteps, void *stream) {
+    zm::BatchParams bp = {};
+    bp.fields = b->d_fields;
+    bp.nfields = (int)b->fields.size();
+    bp.tiles = b->tiles;
+    bp.nsteps = nsteps;
+    for (int i = 0; i < nsteps; i++) bp.step[i] = steps[i];
+    bp.bar = b->d_sync;
+    bp.err = reinterpret_cast<int *>(b->d_sync + 2);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    cudaError_t e = b->dtype == ZM_C128 ? zm::launch_batch_t<double, 8>(bp, b->grid, st)
+                                        : zm::launch_batch_t<float, 16>(bp, b->grid, st);
+    if (e != cudaSuccess)
+        return zm::report_error(ZM_ERR_CUDA, "batch launch: %s (%s)", cudaGetErrorName(e), cudaGetErrorString(e));
+    return ZM_OK;
+}
+
+size_t batch_bytes(zm_batch b) { return (size_t)b->elems * (b->dtype == ZM_C128 ? 16 : 8); }
+
+}  // namespace
+
+extern "C" {
+
+int zm_batch_create(zm_batch *batch, int nfields, const int64_t *n, const int64_t *b, const int64_t *p,
+                    int dtype) {
+    if (!batch) return zm::report_error(ZM_ERR_INVALID_ARG, "batch output pointer is NULL");
+    *batch = nullptr;
+    if (nfields < 1 || nfields > 65536) return zm::report_error(ZM_ERR_INVALID_ARG, "nfields=%d out of range [1, 65536]", nfields);
+    if (!n || !b || !p) return zm::report_error(ZM_ERR_INVALID_ARG, "n, b and p must not be NULL");
+    if (dtype != ZM_C128 && dtype != ZM_C64) return zm::report_error(ZM_ERR_INVALID_ARG, "unknown dtype %d", dtype);
+    const int ept = zm::ept_for(dtype);
+    const int64_t tile_pts = (int64_t)zm::kBatchThreads * ept;
+    zm_batch_s *B = new (std::nothrow) zm_batch_s();
+    if (!B) return zm::report_error(ZM_ERR_NO_MEMORY, "host allocation failed");
+    B->dtype = dtype;
+    cudaGetDevice(&B->device);
+    std::map<std::tuple<int64_t, int64_t, int64_t>, int> seen;
+    int rc = ZM_OK;
+    for (int i = 0; i < nfields && rc == ZM_OK; i++) {
+        if (n[i] < tile_pts / 64 || n[i] > tile_pts) {
+            rc = zm::report_error(ZM_ERR_CONSTRAINT, "field %d: N=%lld outside the batch range [%lld, %lld]", i,
+                                  (long long)n[i], (long long)(tile_pts / 64), (long long)tile_pts);
+            break;
+        }
+        const auto key = std::make_tuple(n[i], b[i], p[i]);
+        auto it = seen.find(key);
+        int pi;
+        if (it == seen.end()) {
+            zm_plan pl = nullptr;
+            rc = zm_plan_create(&pl, 2, n[i], b[i], p[i], dtype, 0);
+            if (rc != ZM_OK) break;
+            pi = (int)B->plans.size();
+            B->plans.push_back(pl);
+            seen.emplace(key, pi);
+        } else {
+            pi = it->second;
+        }
+        const zm_plan_s *pl = B->plans[pi];
+        zm::BatchField f = {};
+        f.g = pl->g;
+        f.off = B->elems;
+        f.tile0 = B->tiles;
+        f.twN = pl->twN;
+        f.T = (int)(tile_pts / n[i]);
+        f.nst_vec = zm::radix_schedule(pl->g.vec, ept, f.rad_vec);
+        f.nst_m = zm::radix_schedule(pl->g.m, ept, f.rad_m);
+        B->fields.push_back(f);
+        B->field_plan.push_back(pi);
+        B->elems += (n[i] * n[i] + 1) & ~int64_t{1};
+        B->tiles += n[i] / f.T;
+    }
+    if (rc == ZM_OK) {
+        B->grid = dtype == ZM_C128 ? zm::batch_grid_t<double, 8>(B->device) : zm::batch_grid_t<float, 16>(B->device);
+        if (B->grid <= 0) rc = zm::report_error(ZM_ERR_CUDA, "batch kernel occupancy query failed");
+    }
+    if (rc == ZM_OK) {
+        const size_t fb = sizeof(zm::BatchField) * B->fields.size();
+        cudaError_t e = cudaMalloc(&B->d_fields, fb);
+        if (e == cudaSuccess) e = cudaMemcpy(B->d_fields, B->fields.data(), fb, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMalloc(&B->d_sync, 4 * sizeof(unsigned));
+        if (e == cudaSuccess) e = cudaMemset(B->d_sync, 0, 4 * sizeof(unsigned));
+        if (e != cudaSuccess)
+            rc = zm::report_error(ZM_ERR_NO_MEMORY, "batch tables: %s", cudaGetErrorString(e));
+    }
+    if (rc != ZM_OK) {
+        zm_batch_destroy(B);
+        return rc;
+    }
+    *batch = B;
+    return ZM_OK;
+}
+
+int zm_batch_destroy(zm_batch batch) {
+    int rc;
+    if ((rc = check_batch(batch))) return rc;
+    for (zm_plan pl : batch->plans) zm_plan_destroy(pl);
+    if (batch->d_fields) cudaFree(batch->d_fields);
+    if (batch->d_sync) cudaFree(batch->d_sync);
+    delete batch;
+    return ZM_OK;
+}
+
+int zm_batch_get_field(zm_batch batch, int i, zm_batch_field *info) {
+    int rc;
+    if ((rc = check_batch(batch))) return rc;
+    if (!info) return zm::report_error(ZM_ERR_INVALID_ARG, "info is NULL");
+    if (i < 0 || i >= (int)batch->fields.size()) return zm::report_error(ZM_ERR_INVALID_ARG, "field %d out of range", i);
+    const zm::BatchField &f = batch->fields[i];
+    info->n = f.g.n;
+    info->b = f.g.b;
+    info->p = f.g.p;
+    info->offset = f.off;
+    info->elems = f.g.n * f.g.n;
+    return ZM_OK;
+}
+
+int zm_batch_total_elems(zm_batch batch, int64_t *elems) {
+    int rc;
+    if ((rc = check_batch(batch))) return rc;
+    if (!elems) return zm::report_error(ZM_ERR_INVALID_ARG, "elems is NULL");
+    *elems = batch->elems;
+    return ZM_OK;
+}
+
+int zm_batch_fill(zm_batch batch, void *data, int kind, uint64_t first_seed, void *stream) {
+    int rc;
+    if ((rc = check_batch(batch)) || (rc = check_buf(data, "data"))) return rc;
+    if (kind != ZM_FIELD_UNIFORM && kind != ZM_FIELD_GAUSSIAN) return zm::report_error(ZM_ERR_INVALID_ARG, "unknown kind %d", kind);
+    zm::BatchStep s = {};
+    s.op = zm::BOP_FILL;
+    s.kind = kind;
+    s.out = data;
+    s.seed = first_seed;
+    return launch(batch, &s, 1, stream);
+}
+
+int zm_batch_forward(zm_batch batch, const void *in, void *out, void *stream) {
+    int rc;
+    if ((rc = check_batch(batch)) || (rc = check_buf(in, "in")) || (rc = check_buf(out, "out"))) return rc;
+    if (overlap_b(in, out, batch_bytes(batch))) return zm::report_error(ZM_ERR_INVALID_ARG, "in and out overlap");
+    zm::BatchStep s[2] = {};
+    s[0].op = zm::BOP_X_FWD; s[0].in = in; s[0].out = out;
+    s[1].op = zm::BOP_Y_FWD; s[1].in = out; s[1].out = out;
+    return launch(batch, s, 2, stream);
+}
+
+int zm_batch_inverse(zm_batch batch, const void *in, void *out, void *work, int normalise, void *stream) {
+    int rc;
+    if ((rc = check_batch(batch)) || (rc = check_buf(in, "in")) || (rc = check_buf(out, "out"))) return rc;
+    const size_t F = batch_bytes(batch);
+    if (overlap_b(in, out, F)) return zm::report_error(ZM_ERR_INVALID_ARG, "in and out overlap");
+    if (work) {
+        if ((rc = check_buf(work, "work"))) return rc;
+        if (overlap_b(work, in, F) || overlap_b(work, out, F))
+            return zm::report_error(ZM_ERR_INVALID_ARG, "work overlaps in/out");
+    }
+    void *tmp = work ? work : const_cast<void *>(in);
+    zm::BatchStep s[2] = {};
+    s[0].op = zm::BOP_Y_INV; s[0].in = in; s[0].out = tmp;
+    s[1].op = zm::BOP_X_INV; s[1].in = tmp; s[1].out = out; s[1].scale = normalise ? 1 : 0;
+    return launch(batch, s, 2, stream);
+}
+
+int zm_batch_poisson(zm_batch batch, const void *rhs, void *phi, void *residual, void *work, double length,
+                     void *stream) {
+    int rc;
+    if ((rc = check_batch(batch)) || (rc = check_buf(rhs, "rhs")) || (rc = check_buf(phi, "phi")) ||
+        (rc = check_buf(work, "work")))
+        return rc;
+    if (residual && (rc = check_buf(residual, "residual"))) return rc;
+    if (!(length > 0.0) || !std::isfinite(length)) return zm::report_error(ZM_ERR_INVALID_ARG, "length must be positive");
+    const size_t F = batch_bytes(batch);
+    if (overlap_b(rhs, phi, F) || overlap_b(rhs, work, F) || overlap_b(phi, work, F) ||
+        (residual && (overlap_b(residual, rhs, F) || overlap_b(residual, phi, F) || overlap_b(residual, work, F))))
+        return zm::report_error(ZM_ERR_INVALID_ARG, "rhs, phi, residual and work must not overlap");
+    zm::BatchStep s[4] = {};
+    const double two_pi = 6.283185307179586476925286766559;
+    s[0].op = zm::BOP_X_FWD; s[0].in = rhs; s[0].out = work;
+    s[1].op = zm::BOP_Y_POISSON; s[1].in = work; s[1].out = work; s[1].a = two_pi / length;
+    s[2].op = zm::BOP_X_INV; s[2].in = work; s[2].out = phi; s[2].scale = 1;
+    int ns = 3;
+    if (residual) {
+        s[3].op = zm::BOP_RESIDUAL; s[3].in = phi; s[3].aux = rhs; s[3].out = residual; s[3].a = 1.0 / length;
+        ns = 4;
+    }
+    return launch(batch, s, ns, stream);
+}
+
+int zm_batch_status(zm_batch batch, int *device_error) {
+    int rc;
+    if ((rc = check_batch(batch))) return rc;
+    if (!device_error) return zm::report_error(ZM_ERR_INVALID_ARG, "device_error is NULL");
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess)
+        return zm::report_error(ZM_ERR_CUDA, "batch status: %s (%s)", cudaGetErrorName(e), cudaGetErrorString(e));
+    int flag = 0;
+    e = cudaMemcpy(&flag, batch->d_sync + 2, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && flag) e = cudaMemset(batch->d_sync, 0, 4 * sizeof(unsigned));
+    if (e != cudaSuccess)
+        return zm::report_error(ZM_ERR_CUDA, "batch status: %s (%s)", cudaGetErrorName(e), cudaGetErrorString(e));
+    *device_error = flag ? 1 : 0;
+    return ZM_OK;
+}
+
+int zm_batch_autotune_b(int64_t n, int64_t p, int dtype, int count, int reps, int64_t *best_b, float *best_ms) {
+    if (count < 1 || reps < 1) return zm::report_error(ZM_ERR_INVALID_ARG, "count and reps must be >= 1");
+    if (n <= 0 || p <= 0 || (n & (n - 1)) || (p & (p - 1)) || n % p)
+        return zm::report_error(ZM_ERR_CONSTRAINT, "N and P must be powers of two with P | N");
+    const int64_t L = n / p;
+    int64_t best = 0;
+    float best_t = 0.f;
+    int rc = ZM_OK;
+    for (int64_t b = 1; b <= L / p && rc == ZM_OK; b *= 2) {
+        std::vector<int64_t> nv(count, n), bv(count, b), pv(count, p);
+        zm_batch bt = nullptr;
+        if (zm_batch_create(&bt, count, nv.data(), bv.data(), pv.data(), dtype) != ZM_OK) continue;   // B not allowed
+        const size_t F = batch_bytes(bt);
+        void *buf = nullptr;
+        cudaError_t e = cudaMalloc(&buf, 4 * F);
+        if (e != cudaSuccess) {
+            zm_batch_destroy(bt);
+            rc = zm::report_error(ZM_ERR_NO_MEMORY, "autotune buffers: %s", cudaGetErrorString(e));
+            break;
+        }
+        char *c = static_cast<char *>(buf);
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        rc = zm_batch_fill(bt, c, ZM_FIELD_GAUSSIAN, 1, nullptr);
+        for (int it = -1; it < reps && rc == ZM_OK; it++) {
+            if (it == 0) cudaEventRecord(e0, nullptr);
+            rc = zm_batch_poisson(bt, c, c + F, c + 2 * F, c + 3 * F, 1.0, nullptr);
+        }
+        cudaEventRecord(e1, nullptr);
+        int flag = 0;
+        if (rc == ZM_OK && (e = cudaEventSynchronize(e1)) != cudaSuccess)
+            rc = zm::report_error(ZM_ERR_CUDA, "autotune timing: %s", cudaGetErrorString(e));
+        if (rc == ZM_OK) rc = zm_batch_status(bt, &flag);
+        if (rc == ZM_OK && flag) rc = zm::report_error(ZM_ERR_TIMEOUT, "autotune: batch barrier timed out");
+        if (rc == ZM_OK) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms /= (float)reps;
+            if (best == 0 || ms < best_t) {
+                best = b;
+                best_t = ms;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaFree(buf);
+        zm_batch_destroy(bt);
+    }
+    if (rc != ZM_OK) return rc;
+    if (best == 0) return zm::report_error(ZM_ERR_CONSTRAINT, "no B is valid for N=%lld", (long long)n);
+    if (best_b) *best_b = best;
+    if (best_ms) *best_ms = best_t;
+    return ZM_OK;
+}
+
+}  // extern "C"

@@ -18,98 +18,13 @@
 // axis pass reads and writes the field exactly once (2F bytes).
 //
 // Sub-transforms are Stockham radix-R stages (R = 2..16) done in place in
-// shared memory: every thread loads its R-point butterflies into registers,
-// the block synchronises, then every thread stores its results.
+// shared memory (zm_tile.cuh): every thread loads its R-point butterflies into
+// registers, the block synchronises, then every thread stores its results.
 #include "zm_common.cuh"
 #include "zm_internal.h"
-#include "zm_lines.cuh"
+#include "zm_tile.cuh"
 
 namespace zm {
-
-// ------------------------------------------------------------ Stockham stage
-// One radix-R stage over all sub-transforms of length n held in shared memory.
-//   COLM = false: sub-transform (t, n1) is the contiguous row s[t*N + n1*VEC + i]
-//   COLM = true:  sub-transform (t, k2) is the column s[t*N + i*VEC + k2]
-// DIR = -1 forward, +1 inverse.  PRETW multiplies the loaded inputs by the
-// inter-step twiddle w_N^{n1 k2} (forward, COLM) or its conjugate (inverse, rows).
-template <int R, int EPT, bool COLM, int DIR, bool PRETW, typename T>
-ZM_DEV void stockham_stage(cpx<T> *s, const Geom &g, int n, int logn, int Ns, int nthr, int tid,
-                           const tw<T> *twN) {
-    constexpr int NB = EPT / R;
-    constexpr bool CONJ = DIR > 0;
-    cpx<T> v[NB][R];
-    int base[NB], jv[NB];
-    const int nR = n / R;
-    const int logR = (R == 2) ? 1 : (R == 4) ? 2 : (R == 8) ? 3 : 4;
-    const int lognR = logn - logR;
-    const int str = COLM ? (int)g.vec : 1;
-#pragma unroll
-    for (int u = 0; u < NB; u++) {
-        const int sig = tid + u * nthr;
-        int j, bb, tagn;  // tagn: the sub-transform's n1 (rows) or k2 (columns)
-        if (!COLM) {
-            j = sig & (nR - 1);
-            const int b = sig >> lognR;              // b = t*M + n1
-            bb = b << g.logVEC;
-            tagn = b & (int)(g.m - 1);
-        } else {
-            const int k2 = sig & (int)(g.vec - 1);
-            const int rest = sig >> g.logVEC;
-            j = rest & (nR - 1);
-            const int t = rest >> lognR;
-            bb = (t << g.logN) + k2;
-            tagn = k2;
-        }
-        base[u] = bb;
-        jv[u] = j;
-#pragma unroll
-        for (int r = 0; r < R; r++) {
-            const int i = j + r * nR;
-            cpx<T> x = s[bb + i * str];
-            if (PRETW) x = twmul<CONJ>(x, ldtw(twN, (int64_t)i * tagn));
-            v[u][r] = x;
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < NB; u++) {
-        const int j = jv[u];
-        const int k = j & (Ns - 1);
-        if (Ns > 1) {
-            // w_{Ns R}^{k r} = w_N^{k r N / (Ns R)}
-            const int sh = g.logN - logn + (logn - __ffs(Ns * R) + 1);
-#pragma unroll
-            for (int r = 1; r < R; r++)
-                v[u][r] = twmul<CONJ>(v[u][r], ldtw(twN, ((int64_t)k * r) << sh));
-        }
-        dft<R, DIR, T>(v[u]);
-        const int idxD = (j - k) * R + k;
-#pragma unroll
-        for (int r = 0; r < R; r++) s[base[u] + (idxD + r * Ns) * str] = v[u][r];
-    }
-    __syncthreads();
-}
-
-template <int EPT, bool COLM, int DIR, typename T>
-ZM_DEV void run_subfft(cpx<T> *s, const Geom &g, int n, int logn, const int *rad, int nst,
-                       bool pretw, int nthr, int tid, const tw<T> *twN) {
-    int Ns = 1;
-    for (int st = 0; st < nst; st++) {
-        const int R = rad[st];
-        const bool pre = pretw && st == 0;
-#define ZM_STAGE(RR)                                                                               \
-    if (pre) stockham_stage<RR, EPT, COLM, DIR, true, T>(s, g, n, logn, Ns, nthr, tid, twN);      \
-    else stockham_stage<RR, EPT, COLM, DIR, false, T>(s, g, n, logn, Ns, nthr, tid, twN);
-        if (R == 2) { ZM_STAGE(2) }
-        else if (R == 4) { ZM_STAGE(4) }
-        else if (R == 8) { ZM_STAGE(8) }
-        else {
-            if constexpr (EPT >= 16) { ZM_STAGE(16) }
-        }
-#undef ZM_STAGE
-        Ns *= R;
-    }
-}
 
 // ------------------------------------------------------------------ kernel
 template <typename T, int EPT, bool INV>
@@ -119,98 +34,20 @@ __global__ void __launch_bounds__(1024) line_fft_kernel(const LineParams prm) {
     __shared__ int64_t s_abase[64], s_fbase[64];
     const Geom &g = prm.g;
     const int nthr = blockDim.x, tid = threadIdx.x;
-    const int TL = prm.T;
-    const int logT = __ffs(TL) - 1;
-    const int64_t l0 = (int64_t)blockIdx.x * TL;
-    const int64_t N = g.n, L = g.L;
     const cpx<T> *in = reinterpret_cast<const cpx<T> *>(prm.in);
     cpx<T> *out = reinterpret_cast<cpx<T> *>(prm.out);
     const tw<T> *twN = reinterpret_cast<const tw<T> *>(prm.twN);
-
-    const LineAddr a0 = line_addr(g, prm.kind, l0);
-    for (int t = tid; t < TL; t += nthr) {
-        const LineAddr a = line_addr(g, prm.kind, l0 + t);
-        s_abase[t] = a.a_base;
-        s_fbase[t] = a.f_base;
-    }
+    const Tile c = tile_begin(g, prm.kind, (int64_t)blockIdx.x * prm.T, prm.T, s_abase, s_fbase, nthr, tid);
     __syncthreads();
-    const int tot = TL << g.logN;
-    const bool f_contig = a0.f_pos == 1;
-
-    // ---------------------------------------------------------------- load
-    if (!INV) {
-        // vector side: line t, chunk c, position pos -> s[t][c*L + pos] = s[t][n1*VEC + n2]
-        for (int e = tid; e < tot; e += nthr) {
-            const int t = e >> g.logN;
-            const int r = e & (int)(N - 1);
-            const int c = r >> g.logL, pos = r & (int)(L - 1);
-            s[e] = ldg(in + s_abase[t] + c * a0.a_chunk + pos);
-        }
-    } else {
-        // frequency side: (t, c, pos = k1*VP + f) -> s[t][k1*VEC + c*VP + f]
-        for (int e = tid; e < tot; e += nthr) {
-            int t, c, pos;
-            if (f_contig) {
-                t = e >> g.logN;
-                const int r = e & (int)(N - 1);
-                c = r >> g.logL; pos = r & (int)(L - 1);
-            } else {
-                t = e & (TL - 1);
-                const int cp = e >> logT;
-                c = cp >> g.logL; pos = cp & (int)(L - 1);
-            }
-            const int k1 = pos >> g.logVP, f = pos & (int)(g.vp - 1);
-            const int si = (t << g.logN) + (k1 << g.logVEC) + (c << g.logVP) + f;
-            s[si] = ldg(in + s_fbase[t] + c * a0.f_chunk + pos * a0.f_pos);
-        }
-    }
+    if (!INV) tile_load_vec(c, g, s, in, nthr, tid);
+    else tile_load_freq(c, g, s, in, nthr, tid);
     __syncthreads();
-
-    // ------------------------------------------------------------- compute
-    if (!prm.permute_only) {
-        if (!INV) {
-            run_subfft<EPT, false, -1, T>(s, g, (int)g.vec, g.logVEC, prm.rad_vec, prm.nst_vec, false,
-                                          nthr, tid, twN);
-            run_subfft<EPT, true, -1, T>(s, g, (int)g.m, g.logM, prm.rad_m, prm.nst_m, true, nthr,
-                                         tid, twN);
-        } else {
-            run_subfft<EPT, true, 1, T>(s, g, (int)g.m, g.logM, prm.rad_m, prm.nst_m, false, nthr,
-                                        tid, twN);
-            run_subfft<EPT, false, 1, T>(s, g, (int)g.vec, g.logVEC, prm.rad_vec, prm.nst_vec, true,
-                                         nthr, tid, twN);
-        }
-    }
-
-    // --------------------------------------------------------------- store
+    if (!prm.permute_only)
+        tile_transform<T, EPT, INV>(s, g, prm.rad_vec, prm.nst_vec, prm.rad_m, prm.nst_m, nthr, tid, twN);
     const bool scl = prm.apply_scale && !prm.permute_only;
-    const T sr = (T)prm.scale_re, si_ = (T)prm.scale_im;
-    if (!INV) {
-        for (int e = tid; e < tot; e += nthr) {
-            int t, c, pos;
-            if (f_contig) {
-                t = e >> g.logN;
-                const int r = e & (int)(N - 1);
-                c = r >> g.logL; pos = r & (int)(L - 1);
-            } else {
-                t = e & (TL - 1);
-                const int cp = e >> logT;
-                c = cp >> g.logL; pos = cp & (int)(L - 1);
-            }
-            const int k1 = pos >> g.logVP, f = pos & (int)(g.vp - 1);
-            cpx<T> v = s[(t << g.logN) + (k1 << g.logVEC) + (c << g.logVP) + f];
-            if (scl) v = {v.x * sr - v.y * si_, v.x * si_ + v.y * sr};
-            out[s_fbase[t] + c * a0.f_chunk + pos * a0.f_pos] = v;
-        }
-    } else {
-        for (int e = tid; e < tot; e += nthr) {
-            const int t = e >> g.logN;
-            const int r = e & (int)(N - 1);
-            const int c = r >> g.logL, pos = r & (int)(L - 1);
-            cpx<T> v = s[e];
-            if (scl) v = {sr * v.x - si_ * v.y, sr * v.y + si_ * v.x};
-            out[s_abase[t] + c * a0.a_chunk + pos] = v;
-        }
-    }
+    const T sr = (T)prm.scale_re, si = (T)prm.scale_im;
+    if (!INV) tile_store_freq(c, g, s, out, scl, sr, si, nthr, tid);
+    else tile_store_vec(c, g, s, out, scl, sr, si, nthr, tid);
 }
 
 // ------------------------------------------------------------------ launch

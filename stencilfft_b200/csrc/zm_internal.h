@@ -9,6 +9,8 @@ namespace zm {
 
 // launch bookkeeping
 void count_launch();
+// radix schedule (remainder radix first, then rmax stages) of a power-of-two length
+int radix_schedule(int64_t n, int rmax, int *rad);
 int max_dyn_smem();
 // record `code` with a formatted message as the calling thread's last error; returns code
 int report_error(int code, const char *fmt, ...);

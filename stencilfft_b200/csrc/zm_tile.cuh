@@ -1,0 +1,216 @@
+// zm_tile.cuh -- one tile of an axis pass with runtime sizes: TL consecutive global
+// lines held in shared memory, Stockham sub-transforms, and the loads / stores between
+// shared memory and the two sides of the pass (see zm_lines.cuh for the addresses).
+//
+// Shared-memory layout of a tile: line t at s[t * N ...]; rows [n1][n2] on the vector
+// side (s[t N + n1 VEC + n2]) and [k1][k2] after the transforms (s[t N + k1 VEC + k2],
+// k2 = c VP + f).  Every function assumes nthr * EPT == TL * N (each thread owns EPT
+// points of every stage) and leaves synchronisation to the caller where noted.
+#pragma once
+
+#include "zm_common.cuh"
+#include "zm_lines.cuh"
+
+namespace zm {
+
+// ------------------------------------------------------------ Stockham stage
+// One radix-R stage over all sub-transforms of length n held in shared memory.
+//   COLM = false: sub-transform (t, n1) is the contiguous row s[t*N + n1*VEC + i]
+//   COLM = true:  sub-transform (t, k2) is the column s[t*N + i*VEC + k2]
+// DIR = -1 forward, +1 inverse.  PRETW multiplies the loaded inputs by the
+// inter-step twiddle w_N^{n1 k2} (forward, COLM) or its conjugate (inverse, rows).
+template <int R, int EPT, bool COLM, int DIR, bool PRETW, typename T>
+ZM_DEV void stockham_stage(cpx<T> *s, const Geom &g, int n, int logn, int Ns, int nthr, int tid,
+                           const tw<T> *twN) {
+    constexpr int NB = EPT / R;
+    constexpr bool CONJ = DIR > 0;
+    cpx<T> v[NB][R];
+    int base[NB], jv[NB];
+    const int nR = n / R;
+    const int logR = (R == 2) ? 1 : (R == 4) ? 2 : (R == 8) ? 3 : 4;
+    const int lognR = logn - logR;
+    const int str = COLM ? (int)g.vec : 1;
+#pragma unroll
+    for (int u = 0; u < NB; u++) {
+        const int sig = tid + u * nthr;
+        int j, bb, tagn;  // tagn: the sub-transform's n1 (rows) or k2 (columns)
+        if (!COLM) {
+            j = sig & (nR - 1);
+            const int b = sig >> lognR;              // b = t*M + n1
+            bb = b << g.logVEC;
+            tagn = b & (int)(g.m - 1);
+        } else {
+            const int k2 = sig & (int)(g.vec - 1);
+            const int rest = sig >> g.logVEC;
+            j = rest & (nR - 1);
+            const int t = rest >> lognR;
+            bb = (t << g.logN) + k2;
+            tagn = k2;
+        }
+        base[u] = bb;
+        jv[u] = j;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int i = j + r * nR;
+            cpx<T> x = s[bb + i * str];
+            if (PRETW) x = twmul<CONJ>(x, ldtw(twN, (int64_t)i * tagn));
+            v[u][r] = x;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < NB; u++) {
+        const int j = jv[u];
+        const int k = j & (Ns - 1);
+        if (Ns > 1) {
+            // w_{Ns R}^{k r} = w_N^{k r N / (Ns R)}
+            const int sh = g.logN - logn + (logn - __ffs(Ns * R) + 1);
+#pragma unroll
+            for (int r = 1; r < R; r++)
+                v[u][r] = twmul<CONJ>(v[u][r], ldtw(twN, ((int64_t)k * r) << sh));
+        }
+        dft<R, DIR, T>(v[u]);
+        const int idxD = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) s[base[u] + (idxD + r * Ns) * str] = v[u][r];
+    }
+    __syncthreads();
+}
+
+template <int EPT, bool COLM, int DIR, typename T>
+ZM_DEV void run_subfft(cpx<T> *s, const Geom &g, int n, int logn, const int *rad, int nst,
+                       bool pretw, int nthr, int tid, const tw<T> *twN) {
+    int Ns = 1;
+    for (int st = 0; st < nst; st++) {
+        const int R = rad[st];
+        const bool pre = pretw && st == 0;
+#define ZM_STAGE(RR)                                                                               \
+    if (pre) stockham_stage<RR, EPT, COLM, DIR, true, T>(s, g, n, logn, Ns, nthr, tid, twN);      \
+    else stockham_stage<RR, EPT, COLM, DIR, false, T>(s, g, n, logn, Ns, nthr, tid, twN);
+        if (R == 2) { ZM_STAGE(2) }
+        else if (R == 4) { ZM_STAGE(4) }
+        else if (R == 8) { ZM_STAGE(8) }
+        else {
+            if constexpr (EPT >= 16) { ZM_STAGE(16) }
+        }
+#undef ZM_STAGE
+        Ns *= R;
+    }
+}
+
+// Both sub-transforms of a tile: forward (VEC-point rows, then the twiddled M-point
+// columns) or inverse (columns, then the conjugate-twiddled rows).  Synchronised.
+template <typename T, int EPT, bool INV>
+ZM_DEV void tile_transform(cpx<T> *s, const Geom &g, const int *rad_vec, int nst_vec,
+                           const int *rad_m, int nst_m, int nthr, int tid, const tw<T> *twN) {
+    if (!INV) {
+        run_subfft<EPT, false, -1, T>(s, g, (int)g.vec, g.logVEC, rad_vec, nst_vec, false, nthr, tid, twN);
+        run_subfft<EPT, true, -1, T>(s, g, (int)g.m, g.logM, rad_m, nst_m, true, nthr, tid, twN);
+    } else {
+        run_subfft<EPT, true, 1, T>(s, g, (int)g.m, g.logM, rad_m, nst_m, false, nthr, tid, twN);
+        run_subfft<EPT, false, 1, T>(s, g, (int)g.vec, g.logVEC, rad_vec, nst_vec, true, nthr, tid, twN);
+    }
+}
+
+// ------------------------------------------------------------ tile addressing
+struct Tile {
+    int TL, logT;
+    int64_t a_chunk, f_chunk, f_pos;
+    bool f_contig;
+    const int64_t *abase, *fbase;   // per line, in shared memory
+};
+
+// Fills the per-line bases (shared arrays of TL entries) of lines l0 .. l0+TL-1 of pass
+// `kind`; the caller synchronises before using the tile.
+ZM_DEV Tile tile_begin(const Geom &g, int kind, int64_t l0, int TL, int64_t *abase, int64_t *fbase,
+                       int nthr, int tid) {
+    const LineAddr a0 = line_addr(g, kind, l0);
+    for (int t = tid; t < TL; t += nthr) {
+        const LineAddr a = line_addr(g, kind, l0 + t);
+        abase[t] = a.a_base;
+        fbase[t] = a.f_base;
+    }
+    Tile c;
+    c.TL = TL;
+    c.logT = __ffs(TL) - 1;
+    c.a_chunk = a0.a_chunk;
+    c.f_chunk = a0.f_chunk;
+    c.f_pos = a0.f_pos;
+    c.f_contig = a0.f_pos == 1;
+    c.abase = abase;
+    c.fbase = fbase;
+    return c;
+}
+
+// element e of the frequency-side sweep -> (t, c, pos); lines fastest where the side is
+// strided so that consecutive threads touch consecutive lines
+ZM_DEV void tile_freq_coords(const Tile &c, const Geom &g, int e, int &t, int &ch, int &pos) {
+    if (c.f_contig) {
+        t = e >> g.logN;
+        const int r = e & (int)(g.n - 1);
+        ch = r >> g.logL;
+        pos = r & (int)(g.L - 1);
+    } else {
+        t = e & (c.TL - 1);
+        const int cp = e >> c.logT;
+        ch = cp >> g.logL;
+        pos = cp & (int)(g.L - 1);
+    }
+}
+
+ZM_DEV int tile_freq_slot(const Geom &g, int t, int ch, int pos) {
+    const int k1 = pos >> g.logVP, f = pos & (int)(g.vp - 1);
+    return (t << g.logN) + (k1 << g.logVEC) + (ch << g.logVP) + f;
+}
+
+// vector side -> rows s[t][c*L + pos] = s[t][n1*VEC + n2]
+template <typename T>
+ZM_DEV void tile_load_vec(const Tile &c, const Geom &g, cpx<T> *s, const cpx<T> *in, int nthr, int tid) {
+    const int tot = c.TL << g.logN;
+    for (int e = tid; e < tot; e += nthr) {
+        const int t = e >> g.logN;
+        const int r = e & (int)(g.n - 1);
+        const int ch = r >> g.logL, pos = r & (int)(g.L - 1);
+        s[e] = ldg(in + c.abase[t] + ch * c.a_chunk + pos);
+    }
+}
+
+// frequency side (t, c, pos = k1*VP + f) -> s[t][k1*VEC + c*VP + f]
+template <typename T>
+ZM_DEV void tile_load_freq(const Tile &c, const Geom &g, cpx<T> *s, const cpx<T> *in, int nthr, int tid) {
+    const int tot = c.TL << g.logN;
+    for (int e = tid; e < tot; e += nthr) {
+        int t, ch, pos;
+        tile_freq_coords(c, g, e, t, ch, pos);
+        s[tile_freq_slot(g, t, ch, pos)] = ldg(in + c.fbase[t] + ch * c.f_chunk + pos * c.f_pos);
+    }
+}
+
+template <typename T>
+ZM_DEV void tile_store_freq(const Tile &c, const Geom &g, const cpx<T> *s, cpx<T> *out, bool scl, T sr,
+                            T si, int nthr, int tid) {
+    const int tot = c.TL << g.logN;
+    for (int e = tid; e < tot; e += nthr) {
+        int t, ch, pos;
+        tile_freq_coords(c, g, e, t, ch, pos);
+        cpx<T> v = s[tile_freq_slot(g, t, ch, pos)];
+        if (scl) v = {v.x * sr - v.y * si, v.x * si + v.y * sr};
+        out[c.fbase[t] + ch * c.f_chunk + pos * c.f_pos] = v;
+    }
+}
+
+template <typename T>
+ZM_DEV void tile_store_vec(const Tile &c, const Geom &g, const cpx<T> *s, cpx<T> *out, bool scl, T sr,
+                           T si, int nthr, int tid) {
+    const int tot = c.TL << g.logN;
+    for (int e = tid; e < tot; e += nthr) {
+        const int t = e >> g.logN;
+        const int r = e & (int)(g.n - 1);
+        const int ch = r >> g.logL, pos = r & (int)(g.L - 1);
+        cpx<T> v = s[e];
+        if (scl) v = {sr * v.x - si * v.y, sr * v.y + si * v.x};
+        out[c.abase[t] + ch * c.a_chunk + pos] = v;
+    }
+}
+
+}  // namespace zm
