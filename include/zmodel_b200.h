@@ -294,6 +294,13 @@ int zm_batch_poisson(zm_batch batch, const void *rhs, void *phi, void *residual,
  * *device_error = 1 when a barrier timed out since the last call. */
 int zm_batch_status(zm_batch batch, int *device_error);
 /*
+ * Failure-detection probe of the batch kernel's grid barrier (no reference counterpart):
+ * one launch whose single barrier waits for `missing` (0 or 1) arrivals more than the
+ * grid has.  With 1 the barrier can never complete: every CTA gives up after the 2 s
+ * limit, the kernel returns and zm_batch_status reports 1.  With 0 it completes.
+ */
+int zm_batch_barrier_probe(zm_batch batch, int missing, void *stream);
+/*
  * B autotuner for batched fields (the reference's compile-time B_DIM knob): times
  * zm_batch_poisson on a batch of `count` fields of size N for every B allowed by the
  * layout constraints (power of two, B | N/P, P | N/(P B)), `reps` timed calls each after

@@ -98,6 +98,7 @@ SIGNATURES = {
     "zm_batch_inverse": [_P, _P, _P, _P, ctypes.c_int, _P],
     "zm_batch_poisson": [_P, _P, _P, _P, _P, _D, _P],
     "zm_batch_status": [_P, ctypes.POINTER(ctypes.c_int)],
+    "zm_batch_barrier_probe": [_P, ctypes.c_int, _P],
     "zm_batch_autotune_b": [_i64, _i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, _PI64,
                             ctypes.POINTER(ctypes.c_float)],
     "zm_last_error_string": [],

@@ -86,6 +86,10 @@ class Batch:
         check(lib().zm_batch_status(self._h, ctypes.byref(v)), "zm_batch_status")
         return v.value
 
+    def barrier_probe(self, missing: int, stream=None) -> None:
+        """Launch the grid-barrier probe (missing = 1: the barrier times out by design)."""
+        check(lib().zm_batch_barrier_probe(self._h, int(missing), _stream_ptr(stream)), "zm_batch_barrier_probe")
+
     @staticmethod
     def autotune_b(n: int, p: int, dtype="c64", count: int = 4, reps: int = 3) -> tuple[int, float]:
         b, ms = ctypes.c_int64(), ctypes.c_float()

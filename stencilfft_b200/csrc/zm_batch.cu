@@ -47,7 +47,8 @@ enum BatchOp : int {
     BOP_X_INV = 3,     // x pass inverse (scale 1/N^2 when step.scale)
     BOP_Y_POISSON = 4, // y pass forward, divide by -|k|^2, y pass inverse (in place)
     BOP_RESIDUAL = 5,  // out = Lap(in) / h^2 - aux (5-point, periodic)
-    BOP_FILL = 6       // out = generator(kind, seed + field) in the real layout
+    BOP_FILL = 6,      // out = generator(kind, seed + field) in the real layout
+    BOP_NOP = 7        // nothing (barrier probe)
 };
 
 struct BatchStep {
@@ -69,6 +70,7 @@ struct BatchParams {
     BatchStep step[kMaxSteps];
     unsigned *bar;     // [0] arrivals, [1] generation
     int *err;          // set to 1 by a barrier that timed out
+    unsigned missing;  // arrivals a barrier waits for beyond the grid (0; > 0 only in the probe)
 };
 
 ZM_DEV unsigned long long globaltimer_ns() {
@@ -142,8 +144,9 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(const BatchPara
     const int tid = threadIdx.x, nthr = blockDim.x;
 
     for (int st = 0; st < bp.nsteps; st++) {
-        if (st > 0 && !grid_barrier(bp.bar, gridDim.x, bp.err, &s_ok)) return;
+        if (st > 0 && !grid_barrier(bp.bar, gridDim.x + bp.missing, bp.err, &s_ok)) return;
         const BatchStep S = bp.step[st];
+        if (S.op == BOP_NOP) continue;
 
         if (S.op == BOP_RESIDUAL || S.op == BOP_FILL) {
             // element-wise steps: field by field, grid-stride inside each field
@@ -311,8 +314,9 @@ bool overlap_b(const void *a, const void *b, size_t bytes) {
     return x < y + bytes && y < x + bytes;
 }
 
-int launch(zm_batch b, const zm::BatchStep *steps, int nsteps, void *stream) {
+int launch(zm_batch b, const zm::BatchStep *steps, int nsteps, void *stream, unsigned missing = 0) {
     zm::BatchParams bp = {};
+    bp.missing = missing;
     bp.fields = b->d_fields;
     bp.nfields = (int)b->fields.size();
     bp.tiles = b->tiles;
@@ -513,6 +517,16 @@ int zm_batch_status(zm_batch batch, int *device_error) {
         return zm::report_error(ZM_ERR_CUDA, "batch status: %s (%s)", cudaGetErrorName(e), cudaGetErrorString(e));
     *device_error = flag ? 1 : 0;
     return ZM_OK;
+}
+
+int zm_batch_barrier_probe(zm_batch batch, int missing, void *stream) {
+    int rc;
+    if ((rc = check_batch(batch))) return rc;
+    if (missing < 0 || missing > 1) return zm::report_error(ZM_ERR_INVALID_ARG, "missing must be 0 or 1");
+    zm::BatchStep s[2] = {};
+    s[0].op = zm::BOP_NOP;
+    s[1].op = zm::BOP_NOP;
+    return launch(batch, s, 2, stream, (unsigned)missing);
 }
 
 int zm_batch_autotune_b(int64_t n, int64_t p, int dtype, int count, int reps, int64_t *best_b, float *best_ms) {

@@ -148,3 +148,27 @@ def test_batching_workload_graph():
         assert e_phi < 1e-5 and e_norm < 1e-5, (n, e_phi, e_norm)
         assert e_res < 1e-6 * n, (n, e_res)   # amplified rounding of phi (see above)
     del graph
+
+
+def test_barrier_timeout_is_reported_not_hung():
+    """Failure detection without a fault: a grid barrier that can never complete (one
+    arrival more than the grid has) gives up after its 2 s limit, the kernel returns,
+    the status reports it, and the context stays usable for the next call."""
+    import time
+
+    from stencilfft_b200 import abi
+    bt = _batch(MIXED[:3], "c64")
+    bt.barrier_probe(0)
+    assert bt.status() == 0
+    t0 = time.perf_counter()
+    bt.barrier_probe(1)
+    assert bt.status() == 1
+    assert time.perf_counter() - t0 < 30
+    assert bt.status() == 0                       # the flag was cleared
+    x, y = bt.empty(), bt.empty()
+    bt.fill(x, abi.ZM_FIELD_GAUSSIAN, 1)
+    bt.forward_fft(x, y)
+    assert bt.status() == 0
+    for i, (n, b, p) in enumerate(MIXED[:3]):
+        xi = to_host(bt.field(x, i))
+        assert relerr(to_host(bt.field(y, i)), O.forward_fft(xi, 2, n, b, p)) < TOL["c64"]
