@@ -9,9 +9,9 @@ VARIANTS = {
         (2, 7): [(1, 16, 512)], (5, 6): [(1, 4, 512)],
         (5, 7): [(1, 2, 512), (2, 2, 256), (2, 4, 512)],
         (4, 8): [(1, 2, 512), (2, 4, 512)],
-        (5, 8): [(2, 2, 512), (1, 1, 512), (2, 1, 256)],
+        (5, 8): [(2, 2, 512), (1, 1, 512), (2, 1, 256), (4, 4, 512), (2, 4, 1024)],
         (6, 7): [(1, 1, 512), (2, 2, 512)],
-        (6, 8): [(4, 2, 512), (2, 1, 512), (1, 1, 1024)],
+        (6, 8): [(4, 2, 512), (2, 1, 512), (1, 1, 1024), (8, 4, 512), (4, 4, 1024), (8, 2, 256)],
     },
     "c128": {
         (4, 4): [(1, 16, 256)], (4, 5): [(1, 8, 256)], (4, 6): [(1, 4, 256)], (2, 7): [(1, 8, 256)],
@@ -41,19 +41,23 @@ for dt, table in VARIANTS.items():
             for (lv, lm), vs in table.items():
                 L.append(f"    case ({lv} << 8) | {lm}: return {len(vs)};")
             L += ["    default: return 0;", "    }", "}", ""]
-            # variants that can run the 2D passes on the pair-interleaved intermediate:
-            # two or more lines per tile (a pair is read and written by one tile, so the
-            # in-place y pass is race-free), two row stages (the vector side moves through
-            # registers, not 16-byte copies) and at least two columns per CTA
-            L += [f"int fused_interleave_ok_{dt}(int logvec, int logm, int variant) {{",
+            # log2 of the widest row interleave G of the 2D intermediate a variant can run
+            # on: G <= 4 lines per tile and G | TL (a group of G rows is read and written
+            # by one tile, so the in-place y pass is race-free), two row stages (the
+            # vector side moves through registers, not 16-byte copies) and at least G
+            # columns per CTA; 0 = plain REPACK layout
+            L += [f"int fused_interleave_lg_{dt}(int logvec, int logm, int variant) {{",
                   "    switch ((logvec << 16) | (logm << 8) | variant) {"]
             for (lv, lm), vs in table.items():
                 for vi, (cl, tl, nt) in enumerate(vs):
                     vec, n = 1 << lv, 1 << (lv + lm)
                     ept = tl * n // (cl * nt)
                     ra2 = vec // min(vec, ept)
-                    if tl >= 2 and ra2 > 1 and vec // cl >= 2:
-                        L.append(f"    case ({lv} << 16) | ({lm} << 8) | {vi}: return 1;")
+                    g = min(tl, 4)
+                    while g > 1 and vec // cl < g:
+                        g //= 2
+                    if g >= 2 and ra2 > 1:
+                        L.append(f"    case ({lv} << 16) | ({lm} << 8) | {vi}: return {g.bit_length() - 1};")
             L += ["    default: return 0;", "    }", "}", ""]
         L += ["}  // namespace zm", ""]
         open(f"zm_fft2_{dt}_{d}.cu", "w").write("\n".join(L))

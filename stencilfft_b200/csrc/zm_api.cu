@@ -161,14 +161,16 @@ static LineParams line_params(const zm_plan_s *p, int kind, const void *in, void
     lp.variant = p->variant;
     lp.permute_only = (p->flags & ZM_FLAG_PERMUTE_ONLY) ? 1 : 0;
     // 2D transforms on the size-specialised passes keep the x -> y intermediate with
-    // pairs of x-frequency rows interleaved (whole 32-byte sectors on both sides).
-    // Both passes of one transform see the same plan state, so they agree on it.
+    // groups of G x-frequency rows interleaved, G up to the tile's line count (at most
+    // 4): the x pass then writes G * TL consecutive elements per line group and the y
+    // pass reads its G lines as one contiguous run.  G <= VP keeps a group inside one
+    // rank chunk.  Both passes of one transform see the same plan state, so they agree.
     lp.lg_inter = 0;
-    if (p->g.dim == 2 && !lp.permute_only && p->nvariants > 0 && p->g.vp >= 2) {
-        const int ok = p->dtype == ZM_C128
-                           ? zm::fused_interleave_ok_c128(p->g.logVEC, p->g.logM, p->variant)
-                           : zm::fused_interleave_ok_c64(p->g.logVEC, p->g.logM, p->variant);
-        lp.lg_inter = ok ? 1 : 0;
+    if (p->g.dim == 2 && !lp.permute_only && p->nvariants > 0) {
+        int lg = p->dtype == ZM_C128 ? zm::fused_interleave_lg_c128(p->g.logVEC, p->g.logM, p->variant)
+                                     : zm::fused_interleave_lg_c64(p->g.logVEC, p->g.logM, p->variant);
+        if (lg > p->g.logVP) lg = p->g.logVP;
+        lp.lg_inter = lg;
     }
     lp.nst_vec = schedule(p->g.vec, p->max_radix, lp.rad_vec);
     lp.nst_m = schedule(p->g.m, p->max_radix, lp.rad_m);

@@ -47,7 +47,7 @@ int fused_variants_c128(int logvec, int logm) {
     }
 }
 
-int fused_interleave_ok_c128(int logvec, int logm, int variant) {
+int fused_interleave_lg_c128(int logvec, int logm, int variant) {
     switch ((logvec << 16) | (logm << 8) | variant) {
     case (5 << 16) | (6 << 8) | 0: return 1;
     case (5 << 16) | (7 << 8) | 1: return 1;

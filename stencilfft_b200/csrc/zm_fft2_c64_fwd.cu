@@ -23,11 +23,16 @@ cudaError_t launch_fused_c64_fwd(const LineParams &prm, cudaStream_t st, bool *h
     case (5 << 16) | (8 << 8) | 0: return launch_fused<float, 5, 8, 2, 2, 512, false>(prm, st);
     case (5 << 16) | (8 << 8) | 1: return launch_fused<float, 5, 8, 1, 1, 512, false>(prm, st);
     case (5 << 16) | (8 << 8) | 2: return launch_fused<float, 5, 8, 2, 1, 256, false>(prm, st);
+    case (5 << 16) | (8 << 8) | 3: return launch_fused<float, 5, 8, 4, 4, 512, false>(prm, st);
+    case (5 << 16) | (8 << 8) | 4: return launch_fused<float, 5, 8, 2, 4, 1024, false>(prm, st);
     case (6 << 16) | (7 << 8) | 0: return launch_fused<float, 6, 7, 1, 1, 512, false>(prm, st);
     case (6 << 16) | (7 << 8) | 1: return launch_fused<float, 6, 7, 2, 2, 512, false>(prm, st);
     case (6 << 16) | (8 << 8) | 0: return launch_fused<float, 6, 8, 4, 2, 512, false>(prm, st);
     case (6 << 16) | (8 << 8) | 1: return launch_fused<float, 6, 8, 2, 1, 512, false>(prm, st);
     case (6 << 16) | (8 << 8) | 2: return launch_fused<float, 6, 8, 1, 1, 1024, false>(prm, st);
+    case (6 << 16) | (8 << 8) | 3: return launch_fused<float, 6, 8, 8, 4, 512, false>(prm, st);
+    case (6 << 16) | (8 << 8) | 4: return launch_fused<float, 6, 8, 4, 4, 1024, false>(prm, st);
+    case (6 << 16) | (8 << 8) | 5: return launch_fused<float, 6, 8, 8, 2, 256, false>(prm, st);
     default: break;
     }
     *handled = false;
@@ -43,22 +48,27 @@ int fused_variants_c64(int logvec, int logm) {
     case (5 << 8) | 6: return 1;
     case (5 << 8) | 7: return 3;
     case (4 << 8) | 8: return 2;
-    case (5 << 8) | 8: return 3;
+    case (5 << 8) | 8: return 5;
     case (6 << 8) | 7: return 2;
-    case (6 << 8) | 8: return 3;
+    case (6 << 8) | 8: return 6;
     default: return 0;
     }
 }
 
-int fused_interleave_ok_c64(int logvec, int logm, int variant) {
+int fused_interleave_lg_c64(int logvec, int logm, int variant) {
     switch ((logvec << 16) | (logm << 8) | variant) {
-    case (5 << 16) | (6 << 8) | 0: return 1;
+    case (5 << 16) | (6 << 8) | 0: return 2;
     case (5 << 16) | (7 << 8) | 0: return 1;
     case (5 << 16) | (7 << 8) | 1: return 1;
-    case (5 << 16) | (7 << 8) | 2: return 1;
+    case (5 << 16) | (7 << 8) | 2: return 2;
     case (5 << 16) | (8 << 8) | 0: return 1;
+    case (5 << 16) | (8 << 8) | 3: return 2;
+    case (5 << 16) | (8 << 8) | 4: return 2;
     case (6 << 16) | (7 << 8) | 1: return 1;
     case (6 << 16) | (8 << 8) | 0: return 1;
+    case (6 << 16) | (8 << 8) | 3: return 2;
+    case (6 << 16) | (8 << 8) | 4: return 2;
+    case (6 << 16) | (8 << 8) | 5: return 1;
     default: return 0;
     }
 }

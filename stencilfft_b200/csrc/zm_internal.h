@@ -28,9 +28,10 @@ cudaError_t launch_fused_c128_fwd(const LineParams &prm, cudaStream_t st, bool *
 cudaError_t launch_fused_c128_inv(const LineParams &prm, cudaStream_t st, bool *handled);
 int fused_variants_c64(int logvec, int logm);
 int fused_variants_c128(int logvec, int logm);
-// 1 when variant `variant` of (VEC, M) supports the pair-interleaved 2D intermediate.
-int fused_interleave_ok_c64(int logvec, int logm, int variant);
-int fused_interleave_ok_c128(int logvec, int logm, int variant);
+// log2 of the widest row interleave of the 2D intermediate variant `variant` of (VEC, M)
+// supports (0 = none).
+int fused_interleave_lg_c64(int logvec, int logm, int variant);
+int fused_interleave_lg_c128(int logvec, int logm, int variant);
 
 // zm_stencil.cu
 enum StencilOp : int { ST_LAPLACE = 0, ST_DX = 1, ST_DY = 2 };
