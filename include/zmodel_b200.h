@@ -90,6 +90,11 @@ int zm_plan_create(zm_plan *plan, int dim, int64_t n, int64_t b, int64_t p, int 
                    unsigned flags);
 int zm_plan_destroy(zm_plan plan);   /* destroy_plans / destroy_buffers (fft_host_plans.h:63, fft.cu:110) */
 int zm_plan_get_info(zm_plan plan, zm_plan_info *info);
+/* Synchronises the device and reports (then clears) the plan's device error word:
+ * *timed_out = 1 when a bounded wait inside one of its kernels (the asynchronous-copy
+ * waits of the persistent FFT passes) gave up since the last call; results computed
+ * since then are not valid.  No reference counterpart. */
+int zm_plan_device_status(zm_plan plan, int *timed_out);
 /* Workspace a transform needs to leave its input untouched (one field, or 0). */
 int zm_plan_workspace_size(zm_plan plan, size_t *bytes);
 /*

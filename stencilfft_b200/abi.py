@@ -60,6 +60,7 @@ SIGNATURES = {
     "zm_plan_destroy": [_P],
     "zm_plan_get_info": [_P, ctypes.POINTER(zm_plan_info)],
     "zm_plan_workspace_size": [_P, ctypes.POINTER(ctypes.c_size_t)],
+    "zm_plan_device_status": [_P, ctypes.POINTER(ctypes.c_int)],
     "zm_plan_kernel_variants": [_P, ctypes.POINTER(ctypes.c_int)],
     "zm_plan_set_kernel_variant": [_P, ctypes.c_int],
     "zm_plan_autotune": [_P, _P, _P, _P, ctypes.c_int, _P, ctypes.POINTER(ctypes.c_int),

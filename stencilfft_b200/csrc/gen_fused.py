@@ -1,6 +1,7 @@
 """Generates zm_fft2_<dtype>_<dir>.cu: the size-specialised fused passes and their
 dispatch tables.  Each (log2 VEC, log2 M) pair lists variants (cluster size CL, lines
-per tile TL, threads NT); the plan's `variant` picks one.  Variant 0, the default, is
+per tile TL, threads NT[, "p" = persistent forward pass with bulk-copy prefetch]); the
+plan's `variant` picks one.  Variant 0, the default, is
 the fastest one measured on B200 at the sizes the table was tuned on; zm_plan_autotune
 re-measures them for a plan."""
 VARIANTS = {
@@ -11,7 +12,7 @@ VARIANTS = {
         (4, 8): [(1, 2, 512), (2, 4, 512)],
         (5, 8): [(2, 2, 512), (1, 1, 512), (2, 1, 256), (4, 4, 512), (2, 4, 1024)],
         (6, 7): [(1, 1, 512), (2, 2, 512)],
-        (6, 8): [(4, 2, 512), (2, 1, 512), (1, 1, 1024), (8, 4, 512), (4, 4, 1024), (8, 2, 256)],
+        (6, 8): [(4, 2, 512), (2, 1, 512), (1, 1, 1024), (8, 4, 512), (4, 4, 1024), (4, 2, 512, "p")],
     },
     "c128": {
         (4, 4): [(1, 16, 256)], (4, 5): [(1, 8, 256)], (4, 6): [(1, 4, 256)], (2, 7): [(1, 8, 256)],
@@ -32,9 +33,11 @@ for dt, table in VARIANTS.items():
              "    *handled = true;",
              "    switch ((prm.g.logVEC << 16) | (prm.g.logM << 8) | prm.variant) {"]
         for (lv, lm), vs in table.items():
-            for vi, (cl, tl, nt) in enumerate(vs):
+            for vi, v in enumerate(vs):
+                cl, tl, nt = v[:3]
+                pers = "true" if len(v) > 3 and v[3] == "p" else "false"
                 L.append(f"    case ({lv} << 16) | ({lm} << 8) | {vi}: "
-                         f"return launch_fused<{T[dt]}, {lv}, {lm}, {cl}, {tl}, {nt}, {'true' if inv else 'false'}>(prm, st);")
+                         f"return launch_fused<{T[dt]}, {lv}, {lm}, {cl}, {tl}, {nt}, {'true' if inv else 'false'}, {pers}>(prm, st);")
         L += ["    default: break;", "    }", "    *handled = false;", "    return cudaSuccess;", "}", ""]
         if not inv:
             L += [f"int fused_variants_{dt}(int logvec, int logm) {{", "    switch ((logvec << 8) | logm) {"]
@@ -49,7 +52,8 @@ for dt, table in VARIANTS.items():
             L += [f"int fused_interleave_lg_{dt}(int logvec, int logm, int variant) {{",
                   "    switch ((logvec << 16) | (logm << 8) | variant) {"]
             for (lv, lm), vs in table.items():
-                for vi, (cl, tl, nt) in enumerate(vs):
+                for vi, v in enumerate(vs):
+                    cl, tl, nt = v[:3]
                     vec, n = 1 << lv, 1 << (lv + lm)
                     ept = tl * n // (cl * nt)
                     ra2 = vec // min(vec, ept)

@@ -160,6 +160,7 @@ static LineParams line_params(const zm_plan_s *p, int kind, const void *in, void
     lp.apply_scale = 0;
     lp.variant = p->variant;
     lp.permute_only = (p->flags & ZM_FLAG_PERMUTE_ONLY) ? 1 : 0;
+    lp.err = p->dev_err;
     // 2D transforms on the size-specialised passes keep the x -> y intermediate with
     // groups of G x-frequency rows interleaved, G up to the tile's line count (at most
     // 4): the x pass then writes G * TL consecutive elements per line group and the y
@@ -292,11 +293,12 @@ int zm_plan_create(zm_plan *plan, int dim, int64_t n, int64_t b, int64_t p, int 
     // inter-step twiddles are generated from it on the device) and the sub-transform
     // tables w_VEC^m, w_M^m.  All four tables share one allocation of 16-byte entries.
     P->twN = P->W = P->twv = P->twm = P->twd = nullptr;
+    P->dev_err = nullptr;
     if (flags & ZM_FLAG_HOST_ONLY) {
         *plan = P;
         return ZM_OK;
     }
-    const int64_t entries = 2 * n + g.vec + g.m;
+    const int64_t entries = 2 * n + g.vec + g.m + 1;   // + one 16-byte slot for the error word
     std::vector<unsigned char> host((size_t)entries * 16);
     const long double pi = 3.141592653589793238462643383279502884L;
     auto put = [&](int64_t slot, int64_t m, int64_t len, bool fp64 = false) {   // w_len^m
@@ -333,6 +335,7 @@ int zm_plan_create(zm_plan *plan, int dim, int64_t n, int64_t b, int64_t p, int 
     P->twd = tb + (size_t)n * 16;
     P->twv = tb + (size_t)2 * n * 16;
     P->twm = tb + (size_t)(2 * n + g.vec) * 16;
+    P->dev_err = reinterpret_cast<int *>(tb + (size_t)(2 * n + g.vec + g.m) * 16);   // zeroed by the upload
     *plan = P;
     return ZM_OK;
 }
@@ -413,6 +416,19 @@ int zm_plan_autotune(zm_plan plan, void *a, void *b, void *work, int reps, void 
     plan->variant = best;
     if (best_variant) *best_variant = best;
     if (best_ms) *best_ms = best_t;
+    return ZM_OK;
+}
+
+int zm_plan_device_status(zm_plan plan, int *timed_out) {
+    int rc;
+    if ((rc = check_device_plan(plan))) return rc;
+    if (!timed_out) return fail(ZM_ERR_INVALID_ARG, "timed_out is NULL");
+    cudaError_t e = cudaDeviceSynchronize();
+    int v = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&v, plan->dev_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && v) e = cudaMemset(plan->dev_err, 0, sizeof(int));
+    if (e != cudaSuccess) return cuda_fail(e, "device status");
+    *timed_out = v ? 1 : 0;
     return ZM_OK;
 }
 

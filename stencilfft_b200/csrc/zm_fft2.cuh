@@ -10,17 +10,22 @@
 //     rows' results are scattered to the owning CTA through distributed shared memory.
 //     With CL = P this is the reference's row / column All-to-All, one CTA per virtual
 //     rank; CL = 1 keeps the whole line in one CTA;
-//   * each CTA's shared memory holds rows X[t][n1][p] (stride VEC + 2) and columns
-//     Y[t][k2][q] (stride M + 1, or one pad per 16 for VEC <= 4) of its slice -- one
-//     buffer, two views used at different times.  The padding keeps the warp access
-//     patterns of every stage (nearly) free of bank conflicts while every register of a
+//   * each CTA's shared memory holds rows X[t][n1][p] and columns Y[t][k2][q] of its
+//     slice -- one buffer, two views used at different times.  Rows are padded by one
+//     element per RA1 points (columns by one per M), which keeps the Stockham write and
+//     read patterns of every stage free of bank conflicts while every register of a
 //     butterfly sits at a compile-time offset from its base;
 //   * each sub-transform is at most two register stages of radix <= 16 (Stockham
 //     indexing), with the stage twiddles w_VEC, w_M in shared memory and the inter-step
-//     twiddle w_N^{n1 k2} read from an [n1][k2]-ordered table, coalesced across lanes;
-//   * the vector side (reference real layout / REPACK layout) moves through shared
-//     memory as 16-byte vectors, all loads of a thread issued before its stores; the
-//     frequency side is read / written straight from registers with lanes along k2.
+//     twiddle w_N^{n1 k2} from an FP64 power walk;
+//   * one tile per cluster, the vector side moved through registers / 16-byte vectors;
+//     or, for forward passes with two row stages in the persistent variants (PERS), a
+//     cluster walks tiles c, c + clusters, ... and each CTA fetches the vector-side rows
+//     of its NEXT tile with bulk asynchronous copies (cp.async.bulk, tracked by an
+//     mbarrier with a bounded wait) into a staging buffer as soon as the current tile's
+//     first row stage has read it, so HBM reads overlap the rest of the tile;
+//   * the frequency side is read / written straight from registers with lanes ordered
+//     so that a warp covers whole sectors.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -38,30 +43,125 @@ template <int CL> ZM_DEV void tile_sync() {
     else __syncthreads();
 }
 
-// Shared-memory geometry of one CTA's slice.
-template <int LV, int LM, int CL, int TL> struct SliceGeom {
-    static constexpr int VEC = 1 << LV, M = 1 << LM;
+// ------------------------------------------------ bulk copies tracked by an mbarrier
+ZM_DEV unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+ZM_DEV void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+ZM_DEV void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+ZM_DEV void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+ZM_DEV bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+ZM_DEV unsigned long long gtimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Wait for the mbarrier phase of the given parity; false after `limit_ns` without it.
+ZM_DEV bool mbar_wait(uint64_t *bar, unsigned parity, unsigned long long limit_ns) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = gtimer_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (gtimer_ns() - t0 > limit_ns) return false;
+    return true;
+}
+// order this thread's earlier generic-proxy shared-memory accesses before its
+// following async-proxy (bulk copy) accesses
+ZM_DEV void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// global -> this CTA's shared memory, `bytes` a multiple of 16, both addresses 16-byte aligned
+ZM_DEV void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"((unsigned long long)__cvta_generic_to_global(src)), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+constexpr unsigned long long kCopyWaitNs = 1000000000ull;   // 1 s
+
+// Shared-memory geometry and radix split of one CTA's slice.
+template <int LV, int LM, int CL, int TL, int NT> struct SliceGeom {
+    static constexpr int VEC = 1 << LV, M = 1 << LM, N = VEC * M;
     static constexpr int ML = M / CL, VL = VEC / CL;
-    static constexpr int XR = VEC + 2;                       // padded row
+    static constexpr int E = TL * N / CL;                    // elements per CTA
+    static constexpr int EPT = E / NT;                       // elements per thread
+    static constexpr int RA1 = VEC < EPT ? VEC : EPT, RA2 = VEC / RA1;
+    static constexpr int RC1 = M < EPT ? M : EPT, RC2 = M / RC1;
+    // rows: with two row stages one pad element per RA1 points (Stockham writes of
+    // RA1 consecutive points by RA2 lanes land in distinct banks); else VEC + 2
+    static constexpr bool PADX = RA2 > 1;
+    static constexpr int XR = PADX ? VEC + RA2 : VEC + 2;
     static constexpr int YP = VEC <= 4 ? 1 : 0;              // pad per 16 in a column
     static constexpr int YR = VEC <= 4 ? M + M / 16 : M + 1; // padded column
     static constexpr int XE = TL * ML * XR, YE = TL * VL * YR;
     static constexpr int ELEMS = XE > YE ? XE : YE;
-    static ZM_DEV int X(int t, int n1l, int p) { return (t * ML + n1l) * XR + p; }
+    static ZM_DEV int X(int t, int n1l, int p) { return (t * ML + n1l) * XR + p + (PADX ? p / RA1 : 0); }
     static ZM_DEV int Y(int t, int k2l, int q) { return (t * VL + k2l) * YR + q + (q >> 4) * YP; }
+    // staging rows of the persistent forward pass: one row of sg interleaved lines
+    // (sg VEC points, a bulk copy each); the stride keeps the first row stage's reads
+    // (lanes over sg lines x RA2 points, then rows) free of bank conflicts
+    static constexpr int SR(int sg) { return sg * VEC + (sg * RA2) % 16; }
+    static constexpr int stage_elems(int sg) { return sg > TL ? 0 : (TL / sg) * ML * SR(sg); }
+    static constexpr int smax(int a, int b) { return a > b ? a : b; }
+    static constexpr int STAGE_ELEMS = smax(stage_elems(1), smax(stage_elems(2), stage_elems(4)));
 };
 
-template <typename T, int LV, int LM, int CL, int TL, int NT, bool INV>
-__global__ void __launch_bounds__(NT, (NT < 1024 ? 1024 / NT : 1)) fused_pass_kernel(const LineParams prm) {
-    using SG = SliceGeom<LV, LM, CL, TL>;
-    constexpr int VEC = SG::VEC, M = SG::M, N = VEC * M;
+template <typename T, int LV, int LM, int CL, int TL, int NT>
+constexpr size_t fused_tables_offset() {
+    return sizeof(cpx<T>) * (size_t)SliceGeom<LV, LM, CL, TL, NT>::ELEMS;
+}
+template <typename T, int LV, int LM, int CL, int TL, int NT>
+constexpr size_t fused_stage_offset() {
+    return fused_tables_offset<T, LV, LM, CL, TL, NT>() +
+           sizeof(tw<T>) * (((size_t)1 << LV) + ((size_t)1 << LM));
+}
+
+// Forward passes with two row stages can run persistent with a staging buffer (PERS,
+// a tile-shape variant of its own) when it fits next to the slice in one CTA's 227 KB
+// of shared memory.
+template <typename T, int LV, int LM, int CL, int TL, int NT, bool INV, bool PERS>
+constexpr bool fused_persistent() {
+    return PERS && !INV && SliceGeom<LV, LM, CL, TL, NT>::RA2 > 1 &&
+           fused_stage_offset<T, LV, LM, CL, TL, NT>() +
+                   sizeof(cpx<T>) * (size_t)SliceGeom<LV, LM, CL, TL, NT>::STAGE_ELEMS <=
+               (size_t)227 * 1024;
+}
+
+template <typename T, int LV, int LM, int CL, int TL, int NT, bool INV, bool PERS>
+constexpr size_t fused_smem_bytes() {
+    return fused_stage_offset<T, LV, LM, CL, TL, NT>() +
+           (fused_persistent<T, LV, LM, CL, TL, NT, INV, PERS>()
+                ? sizeof(cpx<T>) * (size_t)SliceGeom<LV, LM, CL, TL, NT>::STAGE_ELEMS
+                : 0);
+}
+
+// CTAs per SM the register budget is sized for: 1024 / NT threads' worth, or fewer when
+// shared memory cannot hold that many (the persistent passes with their staging buffer)
+template <typename T, int LV, int LM, int CL, int TL, int NT, bool INV, bool PERS>
+constexpr int fused_min_blocks() {
+    constexpr int by_threads = NT < 1024 ? 1024 / NT : 1;
+    constexpr int by_smem = (int)((size_t)228 * 1024 / (fused_smem_bytes<T, LV, LM, CL, TL, NT, INV, PERS>() + 1024));
+    return by_smem < 1 ? 1 : (by_smem < by_threads ? by_smem : by_threads);
+}
+
+template <typename T, int LV, int LM, int CL, int TL, int NT, bool INV, bool PERS>
+__global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, INV, PERS>()))
+    fused_pass_kernel(const LineParams prm) {
+    using SG = SliceGeom<LV, LM, CL, TL, NT>;
+    constexpr int VEC = SG::VEC, M = SG::M;
     constexpr int ML = SG::ML, VL = SG::VL;
-    constexpr int E = TL * N / CL;                    // elements per CTA
-    constexpr int EPT = E / NT;
+    constexpr int E = SG::E, EPT = SG::EPT;
     static_assert(ML >= 1 && VL >= 1 && ML * CL == M && VL * CL == VEC, "cluster split");
     static_assert(EPT * NT == E, "threads must divide the tile");
-    constexpr int RA1 = VEC < EPT ? VEC : EPT, RA2 = VEC / RA1;
-    constexpr int RC1 = M < EPT ? M : EPT, RC2 = M / RC1;
+    constexpr int RA1 = SG::RA1, RA2 = SG::RA2, RC1 = SG::RC1, RC2 = SG::RC2;
     static_assert(RA2 <= EPT && RC2 <= EPT, "sub-transform needs more than two register stages");
     static_assert(EPT % RA1 == 0 && EPT % RA2 == 0 && EPT % RC1 == 0 && EPT % RC2 == 0, "radix");
     constexpr int DIR = INV ? 1 : -1;
@@ -70,30 +170,33 @@ __global__ void __launch_bounds__(NT, (NT < 1024 ? 1024 / NT : 1)) fused_pass_ke
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *S = reinterpret_cast<C *>(smem_raw);
-    Wt *stv = reinterpret_cast<Wt *>(smem_raw + sizeof(C) * SG::ELEMS);   // w_VEC^m, m < VEC
-    Wt *stm = stv + VEC;                                                    // w_M^m,   m < M
+    Wt *stv = reinterpret_cast<Wt *>(smem_raw + fused_tables_offset<T, LV, LM, CL, TL, NT>());  // w_VEC^m
+    Wt *stm = stv + VEC;                                                                          // w_M^m
     __shared__ int64_t s_abase[TL], s_fbase[TL];
+    __shared__ uint64_t s_bar;
 
     int rank = 0;
     if constexpr (CL > 1) rank = (int)cooperative_groups::this_cluster().block_rank();
     const int n1_0 = rank * ML, k2_0 = rank * VL;   // first owned row / column
     const Geom &g = prm.g;
     const int tid = threadIdx.x;
-    const int64_t l0 = (int64_t)(blockIdx.x / CL) * TL;
     const C *in = reinterpret_cast<const C *>(prm.in);
     C *out = reinterpret_cast<C *>(prm.out);
-    const LineAddr a0 = line_addr(g, prm.kind, l0, prm.lg_inter);
-    if (tid < TL) {
-        const LineAddr a = line_addr(g, prm.kind, l0 + tid, prm.lg_inter);
-        s_abase[tid] = a.a_base;
-        s_fbase[tid] = a.f_base;
-    }
+    // strides of the pass (the same for every line)
+    const LineAddr a0 = line_addr(g, prm.kind, 0, prm.lg_inter);
     {
         const Wt *tv = reinterpret_cast<const Wt *>(prm.twv);
         const Wt *tm = reinterpret_cast<const Wt *>(prm.twm);
         for (int i = tid; i < VEC + M; i += NT) stv[i] = i < VEC ? ldtw(tv, i) : ldtw(tm, i - VEC);
     }
-    __syncthreads();
+    // per-line bases of the tile starting at line l0 (the caller synchronises)
+    auto set_tile = [&](int64_t l0) {
+        if (tid < TL) {
+            const LineAddr a = line_addr(g, prm.kind, l0 + tid, prm.lg_inter);
+            s_abase[tid] = a.a_base;
+            s_fbase[tid] = a.f_base;
+        }
+    };
     const int logL = g.logL, logVP = g.logVP;
     const int64_t L = g.L, VP = g.vp;
     const bool scl = prm.apply_scale != 0;
@@ -190,10 +293,194 @@ __global__ void __launch_bounds__(NT, (NT < 1024 ? 1024 / NT : 1)) fused_pass_ke
         return scl ? C{o.x * sre - o.y * sim, o.x * sim + o.y * sre} : o;
     };
 
-    if (!INV) {
-        // ---- 1. vector side -> local rows X (16-byte vectors, all loads before stores);
-        //         with two row stages the first one reads global memory directly instead
-        if constexpr (RA2 == 1) {
+    // ---- forward, second row stage (two row stages): local rows X -> twiddle w_VEC,
+    //      RA2-point transforms, results scattered to the column owners
+    auto fwd_row_stage2_scatter = [&]() {
+        constexpr int NU2 = EPT / RA2;
+        C w[NU2][RA2];
+        int wt[NU2], wn1[NU2], wj[NU2];
+#pragma unroll
+        for (int i = 0; i < NU2; i++) {
+            const int u = tid + i * NT;
+            wj[i] = u & (RA1 - 1);
+            const int rr = u / RA1;
+            wn1[i] = rr % ML;
+            wt[i] = rr / ML;
+#pragma unroll
+            for (int r = 0; r < RA2; r++) w[i][r] = S[SG::X(wt[i], wn1[i], wj[i] + RA1 * r)];
+        }
+#pragma unroll
+        for (int i = 0; i < NU2; i++) {
+#pragma unroll
+            for (int r = 1; r < RA2; r++) w[i][r] = twmul<false>(w[i][r], stv[wj[i] * r]);
+            dft<RA2, DIR, T>(w[i]);
+        }
+        tile_sync<CL>();   // every CTA has finished reading its rows
+#pragma unroll
+        for (int i = 0; i < NU2; i++)
+#pragma unroll
+            for (int r = 0; r < RA2; r++) {
+                const int k2 = wj[i] + RA1 * r;
+                yowner(k2)[SG::Y(wt[i], k2 % VL, n1_0 + wn1[i])] = w[i][r];
+            }
+    };
+
+    // ---- forward: w_N^{n1 k2}, M-point column transforms over n1, frequency-side store
+    auto fwd_columns = [&]() {
+        constexpr int NU = EPT / RC1;
+        C z[NU][RC1];
+        int zt[NU], zk[NU], zj[NU];
+#pragma unroll
+        for (int i = 0; i < NU; i++) {
+            const int u = tid + i * NT;
+            if constexpr (RC2 == 1) {
+                colunit(u, RC2, zt[i], zk[i], zj[i]);   // this stage stores to global
+            } else {
+                zk[i] = u % VL;
+                const int rr = u / VL;
+                zj[i] = rr % RC2;
+                zt[i] = rr / RC2;
+            }
+            Walk wk = walk(zj[i], RC2, k2_0 + zk[i]);               // n1 = zj + RC2 * r
+#pragma unroll
+            for (int r = 0; r < RC1; r++)
+                z[i][r] = twmul<false>(S[SG::Y(zt[i], zk[i], zj[i] + RC2 * r)], wk.next());
+        }
+#pragma unroll
+        for (int i = 0; i < NU; i++) dft<RC1, DIR, T>(z[i]);
+        if constexpr (RC2 == 1) {
+#pragma unroll
+            for (int i = 0; i < NU; i++) {
+                C *op = fptr(out, zt[i], k2_0 + zk[i], 0);
+#pragma unroll
+                for (int r = 0; r < RC1; r++) op[fstep1 * r] = scale_c(z[i][r]);
+            }
+        } else {
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < NU; i++)
+#pragma unroll
+                for (int r = 0; r < RC1; r++) S[SG::Y(zt[i], zk[i], zj[i] * RC1 + r)] = z[i][r];
+            __syncthreads();
+            constexpr int NU2 = EPT / RC2;
+#pragma unroll
+            for (int i = 0; i < NU2; i++) {
+                const int u = tid + i * NT;
+                int t, k2l, j2;
+                colunit(u, RC1, t, k2l, j2);
+                C y[RC2];
+#pragma unroll
+                for (int r = 0; r < RC2; r++) y[r] = S[SG::Y(t, k2l, j2 + RC1 * r)];
+#pragma unroll
+                for (int r = 1; r < RC2; r++) y[r] = twmul<false>(y[r], stm[j2 * r]);
+                dft<RC2, DIR, T>(y);
+                C *op = fptr(out, t, k2_0 + k2l, j2);
+#pragma unroll
+                for (int r = 0; r < RC2; r++) op[fstep2 * r] = scale_c(y[r]);
+            }
+        }
+    };
+
+    if constexpr (fused_persistent<T, LV, LM, CL, TL, NT, INV, PERS>()) {
+        // ================= forward, two row stages: persistent, staged bulk copies
+        C *stage = reinterpret_cast<C *>(smem_raw + fused_stage_offset<T, LV, LM, CL, TL, NT>());
+        const int sg = (int)apos;                       // 1, or the y pass's row interleave
+        const int lgs = sg >= 4 ? 2 : (sg == 2 ? 1 : 0);
+        const int SR = sg >= 4 ? SG::SR(4) : (sg == 2 ? SG::SR(2) : SG::SR(1));
+        const int ncopy = (TL >> lgs) * ML;            // staging rows per tile
+        const unsigned cbytes = (unsigned)(sg * VEC * (int)sizeof(C));
+        const int64_t ntiles = prm.nlines / TL;
+        const int64_t ncl = gridDim.x / CL;
+        if (tid == 0) {
+            mbar_init(&s_bar, 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+        // staging row u = (line group tg, local row n1l) of tile `tile`: sg * VEC
+        // consecutive global elements (the rows of sg interleaved lines)
+        auto issue = [&](int64_t tile) {
+            if (tid == 0) mbar_expect_tx(&s_bar, (unsigned)ncopy * cbytes);
+            __syncthreads();
+            for (int u = tid; u < ncopy; u += NT) {
+                const int tg = u / ML, n1l = u - tg * ML;
+                const LineAddr a = line_addr(g, prm.kind, tile * TL + (tg << lgs), prm.lg_inter);
+                const int r = (n1_0 + n1l) * VEC;
+                const C *src = in + a.a_base + (int64_t)(r >> logL) * a.a_chunk + (int64_t)(r & (L - 1)) * a.a_pos;
+                fence_proxy_async();
+                bulk_g2s(stage + u * SR, src, cbytes, &s_bar);
+            }
+        };
+        unsigned parity = 0;
+        int64_t tile = blockIdx.x / CL;
+        if (tile < ntiles) issue(tile);
+        for (; tile < ntiles; tile += ncl) {
+            __syncthreads();   // the previous tile is done with S and the bases
+            set_tile(tile * TL);
+            if (!mbar_wait(&s_bar, parity, kCopyWaitNs)) {
+                if (prm.err) atomicExch(prm.err, 1);
+                mbar_wait(&s_bar, parity, kCopyWaitNs);   // let copies in flight land, bounded
+            }
+            parity ^= 1u;
+            // first row stage: staging -> RA1-point transforms -> rows X
+            {
+                constexpr int NU = EPT / RA1;
+                C v[NU][RA1];
+                int ut[NU], un1[NU], uj[NU];
+#pragma unroll
+                for (int i = 0; i < NU; i++) {
+                    rowunit(tid + i * NT, RA2, ut[i], un1[i], uj[i]);
+                    const C *row = stage + ((ut[i] >> lgs) * ML + un1[i]) * SR + (uj[i] << lgs) + (ut[i] & (sg - 1));
+#pragma unroll
+                    for (int r = 0; r < RA1; r++) v[i][r] = row[(RA2 * r) << lgs];
+                }
+#pragma unroll
+                for (int i = 0; i < NU; i++) {
+                    dft<RA1, DIR, T>(v[i]);
+#pragma unroll
+                    for (int r = 0; r < RA1; r++) S[SG::X(ut[i], un1[i], uj[i] * RA1 + r)] = v[i][r];
+                }
+            }
+            __syncthreads();   // staging consumed, rows complete, bases visible
+            if (tile + ncl < ntiles) issue(tile + ncl);
+            fwd_row_stage2_scatter();
+            tile_sync<CL>();
+            fwd_columns();
+        }
+        return;
+    } else {
+        set_tile((int64_t)(blockIdx.x / CL) * TL);
+        __syncthreads();
+    }
+
+    if constexpr (!INV && RA2 > 1) {
+        // ================= forward, two row stages, one tile per cluster: the first row
+        // stage reads the vector side straight from global memory
+        {
+            constexpr int NU = EPT / RA1;
+            C v[NU][RA1];
+            int ut[NU], un1[NU], uj[NU];
+#pragma unroll
+            for (int i = 0; i < NU; i++) {
+                rowunit(tid + i * NT, RA2, ut[i], un1[i], uj[i]);
+                const C *row = in + arow(ut[i], un1[i]) + uj[i] * apos;
+#pragma unroll
+                for (int r = 0; r < RA1; r++) v[i][r] = ldg(row + RA2 * r * apos);
+            }
+#pragma unroll
+            for (int i = 0; i < NU; i++) {
+                dft<RA1, DIR, T>(v[i]);
+#pragma unroll
+                for (int r = 0; r < RA1; r++) S[SG::X(ut[i], un1[i], uj[i] * RA1 + r)] = v[i][r];
+            }
+        }
+        __syncthreads();
+        fwd_row_stage2_scatter();
+        tile_sync<CL>();
+        fwd_columns();
+    } else if constexpr (!INV) {
+        // ================= forward, one row stage (RA2 == 1): one tile per cluster
+        // ---- 1. vector side -> local rows X (16-byte vectors, all loads before stores)
+        {
             uint4 buf[VPT];
 #pragma unroll
             for (int i = 0; i < VPT; i++) buf[i] = ldg16(in + aaddr((tid + i * NT) * VE));
@@ -206,140 +493,28 @@ __global__ void __launch_bounds__(NT, (NT < 1024 ? 1024 / NT : 1)) fused_pass_ke
         {
             constexpr int NU = EPT / RA1;
             C v[NU][RA1];
-            int ut[NU], un1[NU], uj[NU];
+            int ut[NU], un1[NU];
 #pragma unroll
             for (int i = 0; i < NU; i++) {
                 const int u = tid + i * NT;
-                if constexpr (RA2 == 1) {
-                    uj[i] = 0;
-                    un1[i] = u % ML;
-                    ut[i] = u / ML;
-                    const C *row = S + SG::X(ut[i], un1[i], 0);
+                un1[i] = u % ML;
+                ut[i] = u / ML;
 #pragma unroll
-                    for (int r = 0; r < RA1; r++) v[i][r] = row[r];
-                } else {
-                    rowunit(u, RA2, ut[i], un1[i], uj[i]);
-                    const C *row = in + arow(ut[i], un1[i]) + uj[i] * apos;
-#pragma unroll
-                    for (int r = 0; r < RA1; r++) v[i][r] = ldg(row + RA2 * r * apos);
-                }
+                for (int r = 0; r < RA1; r++) v[i][r] = S[SG::X(ut[i], un1[i], r)];
             }
 #pragma unroll
             for (int i = 0; i < NU; i++) dft<RA1, DIR, T>(v[i]);
-            if constexpr (RA2 == 1) {
-                tile_sync<CL>();   // every CTA has finished reading its rows
+            tile_sync<CL>();   // every CTA has finished reading its rows
 #pragma unroll
-                for (int i = 0; i < NU; i++)
+            for (int i = 0; i < NU; i++)
 #pragma unroll
-                    for (int r = 0; r < RA1; r++)
-                        yowner(r)[SG::Y(ut[i], r % VL, n1_0 + un1[i])] = v[i][r];
-            } else {
-#pragma unroll
-                for (int i = 0; i < NU; i++) {
-                    C *row = S + SG::X(ut[i], un1[i], uj[i] * RA1);
-#pragma unroll
-                    for (int r = 0; r < RA1; r++) row[r] = v[i][r];
-                }
-                __syncthreads();
-                constexpr int NU2 = EPT / RA2;
-                C w[NU2][RA2];
-                int wt[NU2], wn1[NU2], wj[NU2];
-#pragma unroll
-                for (int i = 0; i < NU2; i++) {
-                    const int u = tid + i * NT;
-                    wj[i] = u & (RA1 - 1);
-                    const int rr = u / RA1;
-                    wn1[i] = rr % ML;
-                    wt[i] = rr / ML;
-                    const C *row = S + SG::X(wt[i], wn1[i], wj[i]);
-#pragma unroll
-                    for (int r = 0; r < RA2; r++) w[i][r] = row[RA1 * r];
-                }
-#pragma unroll
-                for (int i = 0; i < NU2; i++) {
-#pragma unroll
-                    for (int r = 1; r < RA2; r++) w[i][r] = twmul<false>(w[i][r], stv[wj[i] * r]);
-                    dft<RA2, DIR, T>(w[i]);
-                }
-                tile_sync<CL>();
-#pragma unroll
-                for (int i = 0; i < NU2; i++)
-#pragma unroll
-                    for (int r = 0; r < RA2; r++) {
-                        const int k2 = wj[i] + RA1 * r;
-                        yowner(k2)[SG::Y(wt[i], k2 % VL, n1_0 + wn1[i])] = w[i][r];
-                    }
-            }
+                for (int r = 0; r < RA1; r++) yowner(r)[SG::Y(ut[i], r % VL, n1_0 + un1[i])] = v[i][r];
         }
         tile_sync<CL>();
-        // ---- 3. w_N^{n1 k2}, M-point column transforms over n1, frequency-side store
-        {
-            constexpr int NU = EPT / RC1;
-            C z[NU][RC1];
-            int zt[NU], zk[NU], zj[NU];
-#pragma unroll
-            for (int i = 0; i < NU; i++) {
-                const int u = tid + i * NT;
-                if constexpr (RC2 == 1) {
-                    colunit(u, RC2, zt[i], zk[i], zj[i]);   // this stage stores to global
-                } else {
-                    zk[i] = u % VL;
-                    const int rr = u / VL;
-                    zj[i] = rr % RC2;
-                    zt[i] = rr / RC2;
-                }
-                Walk wk = walk(zj[i], RC2, k2_0 + zk[i]);               // n1 = zj + RC2 * r
-                const int yb = SG::Y(zt[i], zk[i], 0);
-#pragma unroll
-                for (int r = 0; r < RC1; r++) {
-                    const int q = zj[i] + RC2 * r;
-                    z[i][r] = twmul<false>(S[yb + q + (q >> 4) * SG::YP], wk.next());
-                }
-            }
-#pragma unroll
-            for (int i = 0; i < NU; i++) dft<RC1, DIR, T>(z[i]);
-            if constexpr (RC2 == 1) {
-#pragma unroll
-                for (int i = 0; i < NU; i++) {
-                    C *op = fptr(out, zt[i], k2_0 + zk[i], 0);
-#pragma unroll
-                    for (int r = 0; r < RC1; r++) op[fstep1 * r] = scale_c(z[i][r]);
-                }
-            } else {
-                __syncthreads();
-#pragma unroll
-                for (int i = 0; i < NU; i++) {
-                    const int yb = SG::Y(zt[i], zk[i], 0);
-#pragma unroll
-                    for (int r = 0; r < RC1; r++) {
-                        const int q = zj[i] * RC1 + r;
-                        S[yb + q + (q >> 4) * SG::YP] = z[i][r];
-                    }
-                }
-                __syncthreads();
-                constexpr int NU2 = EPT / RC2;
-#pragma unroll
-                for (int i = 0; i < NU2; i++) {
-                    const int u = tid + i * NT;
-                    int t, k2l, j2;
-                    colunit(u, RC1, t, k2l, j2);
-                    const int yb = SG::Y(t, k2l, 0);
-                    C y[RC2];
-#pragma unroll
-                    for (int r = 0; r < RC2; r++) {
-                        const int q = j2 + RC1 * r;
-                        y[r] = S[yb + q + (q >> 4) * SG::YP];
-                    }
-#pragma unroll
-                    for (int r = 1; r < RC2; r++) y[r] = twmul<false>(y[r], stm[j2 * r]);
-                    dft<RC2, DIR, T>(y);
-                    C *op = fptr(out, t, k2_0 + k2l, j2);
-#pragma unroll
-                    for (int r = 0; r < RC2; r++) op[fstep2 * r] = scale_c(y[r]);
-                }
-            }
-        }
+        // ---- 3. columns
+        fwd_columns();
     } else {
+        // ================= inverse: one tile per cluster
         // ---- 1. frequency side -> M-point inverse column transforms over k1 (local columns)
         {
             constexpr int NU = EPT / RC1;
@@ -368,14 +543,9 @@ __global__ void __launch_bounds__(NT, (NT < 1024 ? 1024 / NT : 1)) fused_pass_ke
                 }
             } else {
 #pragma unroll
-                for (int i = 0; i < NU; i++) {
-                    const int yb = SG::Y(zt[i], zk[i], 0);
+                for (int i = 0; i < NU; i++)
 #pragma unroll
-                    for (int r = 0; r < RC1; r++) {
-                        const int q = zj[i] * RC1 + r;
-                        S[yb + q + (q >> 4) * SG::YP] = z[i][r];
-                    }
-                }
+                    for (int r = 0; r < RC1; r++) S[SG::Y(zt[i], zk[i], zj[i] * RC1 + r)] = z[i][r];
                 __syncthreads();
                 constexpr int NU2 = EPT / RC2;
                 C y[NU2][RC2];
@@ -387,12 +557,8 @@ __global__ void __launch_bounds__(NT, (NT < 1024 ? 1024 / NT : 1)) fused_pass_ke
                     const int rr = u / VL;
                     yj[i] = rr % RC1;
                     yt[i] = rr / RC1;
-                    const int yb = SG::Y(yt[i], yk[i], 0);
 #pragma unroll
-                    for (int r = 0; r < RC2; r++) {
-                        const int q = yj[i] + RC1 * r;
-                        y[i][r] = S[yb + q + (q >> 4) * SG::YP];
-                    }
+                    for (int r = 0; r < RC2; r++) y[i][r] = S[SG::Y(yt[i], yk[i], yj[i] + RC1 * r)];
                 }
 #pragma unroll
                 for (int i = 0; i < NU2; i++) {
@@ -426,27 +592,17 @@ __global__ void __launch_bounds__(NT, (NT < 1024 ? 1024 / NT : 1)) fused_pass_ke
                 const int rr = u / RA2;
                 un1[i] = rr % ML;
                 ut[i] = rr / ML;
-                const C *row = S + SG::X(ut[i], un1[i], uj[i]);
 #pragma unroll
-                for (int r = 0; r < RA1; r++) v[i][r] = row[RA2 * r];
+                for (int r = 0; r < RA1; r++) v[i][r] = S[SG::X(ut[i], un1[i], uj[i] + RA2 * r)];
             }
             __syncthreads();
 #pragma unroll
             for (int i = 0; i < NU; i++) dft<RA1, DIR, T>(v[i]);
-            if constexpr (RA2 == 1) {
 #pragma unroll
-                for (int i = 0; i < NU; i++) {
-                    C *row = S + SG::X(ut[i], un1[i], 0);
+            for (int i = 0; i < NU; i++)
 #pragma unroll
-                    for (int r = 0; r < RA1; r++) row[r] = v[i][r];
-                }
-            } else {
-#pragma unroll
-                for (int i = 0; i < NU; i++) {
-                    C *row = S + SG::X(ut[i], un1[i], uj[i] * RA1);
-#pragma unroll
-                    for (int r = 0; r < RA1; r++) row[r] = v[i][r];
-                }
+                for (int r = 0; r < RA1; r++) S[SG::X(ut[i], un1[i], uj[i] * RA1 + r)] = v[i][r];
+            if constexpr (RA2 > 1) {
                 __syncthreads();
                 constexpr int NU2 = EPT / RA2;
                 C w[NU2][RA2];
@@ -455,9 +611,8 @@ __global__ void __launch_bounds__(NT, (NT < 1024 ? 1024 / NT : 1)) fused_pass_ke
                 for (int i = 0; i < NU2; i++) {
                     const int u = tid + i * NT;
                     rowunit(u, RA1, wt[i], wn1[i], wj[i]);   // this stage stores to global
-                    const C *row = S + SG::X(wt[i], wn1[i], wj[i]);
 #pragma unroll
-                    for (int r = 0; r < RA2; r++) w[i][r] = row[RA1 * r];
+                    for (int r = 0; r < RA2; r++) w[i][r] = S[SG::X(wt[i], wn1[i], wj[i] + RA1 * r)];
                 }
 #pragma unroll
                 for (int i = 0; i < NU2; i++) {
@@ -492,25 +647,54 @@ __global__ void __launch_bounds__(NT, (NT < 1024 ? 1024 / NT : 1)) fused_pass_ke
     }
 }
 
-template <typename T, int LV, int LM, int CL, int TL, int NT>
-constexpr size_t fused_smem_bytes() {
-    return sizeof(cpx<T>) * (size_t)SliceGeom<LV, LM, CL, TL>::ELEMS +
-           sizeof(tw<T>) * (((size_t)1 << LV) + ((size_t)1 << LM));
+// Clusters (or CTAs) resident at once for a persistent launch of `kern`, per device.
+template <int CL, int NT, typename K>
+static int resident_clusters(K kern, size_t smem, int dev) {
+    int n = 0;
+    if constexpr (CL == 1) {
+        int per_sm = 0, sms = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem) != cudaSuccess) return 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+        n = per_sm * sms;
+    } else {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(CL);
+        cfg.blockDim = dim3(NT);
+        cfg.dynamicSmemBytes = smem;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = CL;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess) return 0;
+    }
+    return n;
 }
 
-template <typename T, int LV, int LM, int CL, int TL, int NT, bool INV>
+template <typename T, int LV, int LM, int CL, int TL, int NT, bool INV, bool PERS = false>
 cudaError_t launch_fused(const LineParams &prm, cudaStream_t st) {
-    constexpr size_t smem = fused_smem_bytes<T, LV, LM, CL, TL, NT>();
-    auto kern = fused_pass_kernel<T, LV, LM, CL, TL, NT, INV>;
-    static int attr_done[64];
+    constexpr size_t smem = fused_smem_bytes<T, LV, LM, CL, TL, NT, INV, PERS>();
+    static_assert(smem <= 227 * 1024, "shared memory of one CTA");
+    constexpr bool persistent = fused_persistent<T, LV, LM, CL, TL, NT, INV, PERS>();
+    auto kern = fused_pass_kernel<T, LV, LM, CL, TL, NT, INV, PERS>;
+    static int attr_done[64], clusters[64];
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 64 && !attr_done[dev]) {
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!attr_done[dev]) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
+        if (persistent) {
+            clusters[dev] = resident_clusters<CL, NT>(kern, smem, dev);
+            if (clusters[dev] <= 0) return cudaErrorInvalidConfiguration;
+        }
         attr_done[dev] = 1;
     }
-    const unsigned grid = (unsigned)(prm.nlines / TL) * CL;
+    const int64_t ntiles = prm.nlines / TL;
+    const int64_t nclus = persistent ? (ntiles < clusters[dev] ? ntiles : clusters[dev]) : ntiles;
+    const unsigned grid = (unsigned)nclus * CL;
     if constexpr (CL == 1) {
         kern<<<grid, NT, smem, st>>>(prm);
     } else {

@@ -9,22 +9,22 @@ namespace zm {
 cudaError_t launch_fused_c128_fwd(const LineParams &prm, cudaStream_t st, bool *handled) {
     *handled = true;
     switch ((prm.g.logVEC << 16) | (prm.g.logM << 8) | prm.variant) {
-    case (4 << 16) | (4 << 8) | 0: return launch_fused<double, 4, 4, 1, 16, 256, false>(prm, st);
-    case (4 << 16) | (5 << 8) | 0: return launch_fused<double, 4, 5, 1, 8, 256, false>(prm, st);
-    case (4 << 16) | (6 << 8) | 0: return launch_fused<double, 4, 6, 1, 4, 256, false>(prm, st);
-    case (2 << 16) | (7 << 8) | 0: return launch_fused<double, 2, 7, 1, 8, 256, false>(prm, st);
-    case (5 << 16) | (6 << 8) | 0: return launch_fused<double, 5, 6, 1, 2, 256, false>(prm, st);
-    case (5 << 16) | (7 << 8) | 0: return launch_fused<double, 5, 7, 1, 1, 256, false>(prm, st);
-    case (5 << 16) | (7 << 8) | 1: return launch_fused<double, 5, 7, 2, 2, 256, false>(prm, st);
-    case (4 << 16) | (8 << 8) | 0: return launch_fused<double, 4, 8, 1, 1, 256, false>(prm, st);
-    case (4 << 16) | (8 << 8) | 1: return launch_fused<double, 4, 8, 2, 2, 256, false>(prm, st);
-    case (5 << 16) | (8 << 8) | 0: return launch_fused<double, 5, 8, 1, 1, 512, false>(prm, st);
-    case (5 << 16) | (8 << 8) | 1: return launch_fused<double, 5, 8, 2, 1, 256, false>(prm, st);
-    case (6 << 16) | (7 << 8) | 0: return launch_fused<double, 6, 7, 2, 1, 256, false>(prm, st);
-    case (6 << 16) | (7 << 8) | 1: return launch_fused<double, 6, 7, 1, 1, 512, false>(prm, st);
-    case (6 << 16) | (8 << 8) | 0: return launch_fused<double, 6, 8, 2, 1, 512, false>(prm, st);
-    case (6 << 16) | (8 << 8) | 1: return launch_fused<double, 6, 8, 4, 1, 256, false>(prm, st);
-    case (6 << 16) | (8 << 8) | 2: return launch_fused<double, 6, 8, 4, 2, 512, false>(prm, st);
+    case (4 << 16) | (4 << 8) | 0: return launch_fused<double, 4, 4, 1, 16, 256, false, false>(prm, st);
+    case (4 << 16) | (5 << 8) | 0: return launch_fused<double, 4, 5, 1, 8, 256, false, false>(prm, st);
+    case (4 << 16) | (6 << 8) | 0: return launch_fused<double, 4, 6, 1, 4, 256, false, false>(prm, st);
+    case (2 << 16) | (7 << 8) | 0: return launch_fused<double, 2, 7, 1, 8, 256, false, false>(prm, st);
+    case (5 << 16) | (6 << 8) | 0: return launch_fused<double, 5, 6, 1, 2, 256, false, false>(prm, st);
+    case (5 << 16) | (7 << 8) | 0: return launch_fused<double, 5, 7, 1, 1, 256, false, false>(prm, st);
+    case (5 << 16) | (7 << 8) | 1: return launch_fused<double, 5, 7, 2, 2, 256, false, false>(prm, st);
+    case (4 << 16) | (8 << 8) | 0: return launch_fused<double, 4, 8, 1, 1, 256, false, false>(prm, st);
+    case (4 << 16) | (8 << 8) | 1: return launch_fused<double, 4, 8, 2, 2, 256, false, false>(prm, st);
+    case (5 << 16) | (8 << 8) | 0: return launch_fused<double, 5, 8, 1, 1, 512, false, false>(prm, st);
+    case (5 << 16) | (8 << 8) | 1: return launch_fused<double, 5, 8, 2, 1, 256, false, false>(prm, st);
+    case (6 << 16) | (7 << 8) | 0: return launch_fused<double, 6, 7, 2, 1, 256, false, false>(prm, st);
+    case (6 << 16) | (7 << 8) | 1: return launch_fused<double, 6, 7, 1, 1, 512, false, false>(prm, st);
+    case (6 << 16) | (8 << 8) | 0: return launch_fused<double, 6, 8, 2, 1, 512, false, false>(prm, st);
+    case (6 << 16) | (8 << 8) | 1: return launch_fused<double, 6, 8, 4, 1, 256, false, false>(prm, st);
+    case (6 << 16) | (8 << 8) | 2: return launch_fused<double, 6, 8, 4, 2, 512, false, false>(prm, st);
     default: break;
     }
     *handled = false;

@@ -41,6 +41,7 @@ struct LineParams {
     int variant;       // tile-shape variant of the size-specialised kernel (0 = default)
     int permute_only;  // skip all arithmetic (reference do_compute=false)
     int lg_inter;      // 2D: log2 of the row interleave of the x -> y intermediate (0 = plain REPACK layout)
+    int *err;          // device word set to 1 when a bounded wait inside a kernel gives up
     // radix schedules of the two sub-transforms (first stage first)
     int nst_vec, nst_m;
     int rad_vec[8], rad_m[8];
@@ -64,4 +65,5 @@ struct zm_plan_s {
     int max_radix;
     int variant;      // tile-shape variant of the size-specialised kernel
     int nvariants;    // variants available for (VEC, M, dtype); 0 = runtime-sized kernel only
+    int *dev_err;     // device error word (bounded waits that gave up), inside the tables allocation
 };

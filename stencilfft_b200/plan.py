@@ -106,6 +106,12 @@ class Plan:
     def set_kernel_variant(self, variant: int) -> None:
         check(lib().zm_plan_set_kernel_variant(self._h, int(variant)), "zm_plan_set_kernel_variant")
 
+    def device_status(self) -> int:
+        """Synchronise; 1 if a bounded wait in one of this plan's kernels gave up (cleared)."""
+        v = ctypes.c_int()
+        check(lib().zm_plan_device_status(self._h, ctypes.byref(v)), "zm_plan_device_status")
+        return v.value
+
     def autotune(self, a, b, work=None, reps: int = 3, stream=None) -> tuple[int, float]:
         """Time a forward + inverse round trip per kernel variant and keep the fastest.
 
