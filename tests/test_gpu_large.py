@@ -67,6 +67,7 @@ def test_every_kernel_variant_full_size(n, b, p, dt):
         assert _norm(spec - exp) / _norm(exp) < tol, v
         pl.inverse_fft(spec, back, scale=1.0 / (n * n), work=work)
         assert _norm(back - u) / _norm(u) < tol, v
+    assert pl.device_status() == 0   # no bounded wait gave up (persistent variants)
 
 
 @pytest.mark.parametrize("n,b,p,dt", LARGE)
