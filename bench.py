@@ -125,6 +125,17 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def max_over_ranks(value: float, dist=None, device: str = "cuda") -> float:
+    """The largest `value` over all ranks of the default process group (itself when
+    there is none).  Every rank must call it at the same point."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ------------------------------------------------------------------ CPU arm
 
 def cpu_sample(threads: int | None = None):
@@ -291,11 +302,7 @@ def run_ours(args, rank: int, world: int):
     torch.cuda.empty_cache()
 
     def gmax(v: float) -> float:
-        if not dist:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(v, dist, "cuda")
 
     ms = gmax(main["ms"])
     e2e_ms = gmax(main["e2e_ms"])

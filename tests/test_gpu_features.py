@@ -188,3 +188,38 @@ def test_autotune_keeps_results(dt):
     a = to_dev(x, dt)
     pl.forward_fft(a, bb, work=w)
     assert relerr(to_host(bb), O.forward_fft(x, 2, n, b, p)) < TOL[dt]
+
+
+@pytest.mark.parametrize("dt", ["c64", "c128"])
+def test_calls_capture_in_cuda_graph(dt):
+    """No call allocates or synchronises: forward -> spectral op -> inverse -> Laplacian
+    captured in a CUDA graph and replayed gives the eager results bit for bit."""
+    import torch
+    from stencilfft_b200 import abi, launch_count
+    n, b, p = 1024, 32, 4
+    pl = _plan(2, n, b, p, dt)
+    u = pl.empty()
+    pl.fill(u, abi.ZM_FIELD_GAUSSIAN, 21)
+    spec, back, lap, work = pl.empty(), pl.empty(), pl.empty(), pl.empty()
+
+    def chain():
+        pl.forward_fft(u, spec, work=work)
+        pl.spectral_apply(spec, abi.ZM_SPECTRAL_GAUSSIAN, n / 16)
+        pl.inverse_fft(spec, back, scale=1.0 / n ** 2, work=work)
+        pl.laplace(back, lap)
+
+    chain()
+    torch.cuda.synchronize()
+    eager = lap.clone()
+    lap.zero_()
+    stream = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        chain()
+    l0 = launch_count()
+    graph.replay()
+    torch.cuda.synchronize()
+    assert launch_count() == l0
+    assert torch.equal(lap, eager)
+    assert pl.device_status() == 0
+    del graph
