@@ -39,9 +39,11 @@ def _ptr(t) -> int:
 class Plan:
     """Immutable description of an N^dim field on a P^dim virtual-rank grid with B x B blocks."""
 
-    def __init__(self, dim: int, n: int, b: int, p: int, dtype="c128", permute_only: bool = False):
+    def __init__(self, dim: int, n: int, b: int, p: int, dtype="c128", permute_only: bool = False,
+                 host_only: bool = False):
+        """host_only: no device resources (ZM_FLAG_HOST_ONLY) -- sizes and index maps only."""
         self._h = ctypes.c_void_p()
-        flags = abi.ZM_FLAG_PERMUTE_ONLY if permute_only else 0
+        flags = (abi.ZM_FLAG_PERMUTE_ONLY if permute_only else 0) | (abi.ZM_FLAG_HOST_ONLY if host_only else 0)
         if dtype not in _DT:
             raise ValueError(f"dtype must be 'c128' or 'c64', got {dtype!r}")
         check(lib().zm_plan_create(ctypes.byref(self._h), int(dim), int(n), int(b), int(p),
