@@ -117,6 +117,16 @@ int zm_plan_set_kernel_variant(zm_plan plan, int variant);
  */
 int zm_plan_autotune(zm_plan plan, void *a, void *b, void *work, int reps, void *stream,
                      int *best_variant, float *best_ms);
+/*
+ * B autotuner (the reference's compile-time B_DIM, chosen here per size): for every B
+ * the layout constraints allow (power of two, B | N/P, P | N/(P B)) creates a plan,
+ * fills a seeded field and runs zm_plan_autotune on it; returns the B, kernel variant
+ * and round-trip time of the fastest.  Allocates and frees three fields of its own and
+ * synchronises the device.  Note that B fixes the layout: data must be produced in the
+ * layout of the chosen B.
+ */
+int zm_autotune_b(int dim, int64_t n, int64_t p, int dtype, int reps, int64_t *best_b, int *best_variant,
+                  float *best_ms);
 
 /*
  * Transforms over all virtual ranks.

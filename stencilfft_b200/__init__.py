@@ -12,7 +12,7 @@ fallback -- calls fail loudly when the CUDA library is missing.
 from .abi import (ZM_C128, ZM_C64, ZM_FLAG_PERMUTE_ONLY, ZmError, lib, library_path,  # noqa: F401
                   launch_count)
 from .batch import Batch  # noqa: F401
-from .plan import Plan  # noqa: F401
+from .plan import Plan, autotune_b  # noqa: F401
 
-__all__ = ["Plan", "Batch", "ZmError", "ZM_C128", "ZM_C64", "ZM_FLAG_PERMUTE_ONLY", "lib", "library_path",
+__all__ = ["Plan", "Batch", "autotune_b", "ZmError", "ZM_C128", "ZM_C64", "ZM_FLAG_PERMUTE_ONLY", "lib", "library_path",
            "launch_count"]

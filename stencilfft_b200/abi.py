@@ -63,6 +63,8 @@ SIGNATURES = {
     "zm_plan_device_status": [_P, ctypes.POINTER(ctypes.c_int)],
     "zm_plan_kernel_variants": [_P, ctypes.POINTER(ctypes.c_int)],
     "zm_plan_set_kernel_variant": [_P, ctypes.c_int],
+    "zm_autotune_b": [ctypes.c_int, _i64, _i64, ctypes.c_int, ctypes.c_int, _PI64, ctypes.POINTER(ctypes.c_int),
+                      ctypes.POINTER(ctypes.c_float)],
     "zm_plan_autotune": [_P, _P, _P, _P, ctypes.c_int, _P, ctypes.POINTER(ctypes.c_int),
                          ctypes.POINTER(ctypes.c_float)],
     "zm_fft_forward": [_P, _P, _P, _P, _P],

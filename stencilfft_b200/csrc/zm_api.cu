@@ -419,6 +419,46 @@ int zm_plan_autotune(zm_plan plan, void *a, void *b, void *work, int reps, void 
     return ZM_OK;
 }
 
+int zm_autotune_b(int dim, int64_t n, int64_t p, int dtype, int reps, int64_t *best_b, int *best_variant,
+                  float *best_ms) {
+    if (reps < 1) return fail(ZM_ERR_INVALID_ARG, "reps must be >= 1 (got %d)", reps);
+    if (dim != 2 && dim != 3) return fail(ZM_ERR_INVALID_ARG, "dim must be 2 or 3 (got %d)", dim);
+    if (!pow2(n) || !pow2(p) || n % p) return fail(ZM_ERR_CONSTRAINT, "N and P must be powers of two with P | N");
+    const int64_t L = n / p;
+    int64_t bb = 0;
+    int bv = 0;
+    float bms = 0.f;
+    for (int64_t b = 1; b <= L / p; b *= 2) {
+        zm_plan pl = nullptr;
+        if (zm_plan_create(&pl, dim, n, b, p, dtype, 0) != ZM_OK) continue;   // B outside the constraints
+        const size_t F = pl->total * pl->elem_bytes;
+        void *buf = nullptr;
+        cudaError_t e = cudaMalloc(&buf, 3 * F);
+        if (e != cudaSuccess) {
+            zm_plan_destroy(pl);
+            return fail(ZM_ERR_NO_MEMORY, "autotune buffers (%zu bytes): %s", 3 * F, cudaGetErrorString(e));
+        }
+        char *c = static_cast<char *>(buf);
+        int v = 0;
+        float ms = 0.f;
+        int rc = zm_fill_field(pl, c, ZM_FIELD_GAUSSIAN, 1, nullptr);
+        if (rc == ZM_OK) rc = zm_plan_autotune(pl, c, c + F, c + 2 * F, reps, nullptr, &v, &ms);
+        cudaFree(buf);
+        zm_plan_destroy(pl);
+        if (rc != ZM_OK) return rc;
+        if (bb == 0 || ms < bms) {
+            bb = b;
+            bv = v;
+            bms = ms;
+        }
+    }
+    if (bb == 0) return fail(ZM_ERR_CONSTRAINT, "no B is valid for N=%lld, P=%lld", (long long)n, (long long)p);
+    if (best_b) *best_b = bb;
+    if (best_variant) *best_variant = bv;
+    if (best_ms) *best_ms = bms;
+    return ZM_OK;
+}
+
 int zm_plan_device_status(zm_plan plan, int *timed_out) {
     int rc;
     if ((rc = check_device_plan(plan))) return rc;

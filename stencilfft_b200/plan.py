@@ -296,3 +296,12 @@ class Plan:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def autotune_b(dim: int, n: int, p: int, dtype="c64", reps: int = 2) -> tuple[int, int, float]:
+    """Fastest (B, kernel variant, ms per forward + inverse round trip) for an N^dim field
+    on a P^dim grid (zm_autotune_b)."""
+    b, v, ms = ctypes.c_int64(), ctypes.c_int(), ctypes.c_float()
+    check(lib().zm_autotune_b(int(dim), int(n), int(p), _DT[dtype], int(reps), ctypes.byref(b), ctypes.byref(v),
+                              ctypes.byref(ms)), "zm_autotune_b")
+    return b.value, v.value, ms.value

@@ -223,3 +223,19 @@ def test_calls_capture_in_cuda_graph(dt):
     assert torch.equal(lap, eager)
     assert pl.device_status() == 0
     del graph
+
+
+def test_autotune_b_picks_a_valid_layout():
+    """zm_autotune_b: the chosen B satisfies the layout constraints and a plan with it
+    transforms correctly."""
+    from stencilfft_b200 import Plan, autotune_b
+    n, p = 1024, 2
+    b, v, ms = autotune_b(2, n, p, "c64", reps=1)
+    L = n // p
+    assert b >= 1 and L % b == 0 and (L // b) % p == 0 and ms > 0
+    pl = Plan(2, n, b, p, dtype="c64")
+    assert 0 <= v < max(1, pl.kernel_variants)
+    x = O.natural_to_real_layout(rand_field(2, n, 8), b, p)
+    out = pl.empty()
+    pl.forward_fft(to_dev(x, "c64"), out, work=pl.empty())
+    assert relerr(to_host(out), O.forward_fft(x, 2, n, b, p)) < TOL["c64"]
