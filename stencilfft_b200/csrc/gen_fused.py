@@ -21,6 +21,15 @@ VARIANTS = {
         (6, 8): [(2, 1, 512), (4, 1, 256), (4, 2, 512)],
     },
 }
+# Out-of-place 2D forward configurations (used when the caller passes a workspace and the
+# plan runs its default variant): x pass variant, y pass variant, log2 of the row
+# interleave of the intermediate.  Measured on B200 at N = 16384, P = 4, B = 64 (c64):
+# one 1024-thread CTA per line in both passes with 8-row interleave, 3.73 ms per forward
+# transform against 4.61 for the in-place default.
+FWD_OOP = {
+    "c64": {(6, 8): (2, 2, 3)},
+    "c128": {},
+}
 T = {"c64": "float", "c128": "double"}
 for dt, table in VARIANTS.items():
     for inv in (False, True):
@@ -62,6 +71,11 @@ for dt, table in VARIANTS.items():
                         g //= 2
                     if g >= 2 and ra2 > 1:
                         L.append(f"    case ({lv} << 16) | ({lm} << 8) | {vi}: return {g.bit_length() - 1};")
+            L += ["    default: return 0;", "    }", "}", ""]
+            L += [f"int fused_fwd_oop_{dt}(int logvec, int logm, int *vx, int *vy, int *lg) {{",
+                  "    switch ((logvec << 8) | logm) {"]
+            for (lv, lm), (vx, vy, lg) in FWD_OOP[dt].items():
+                L.append(f"    case ({lv} << 8) | {lm}: *vx = {vx}; *vy = {vy}; *lg = {lg}; return 1;")
             L += ["    default: return 0;", "    }", "}", ""]
         L += ["}  // namespace zm", ""]
         open(f"zm_fft2_{dt}_{d}.cu", "w").write("\n".join(L))

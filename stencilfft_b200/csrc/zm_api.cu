@@ -178,9 +178,24 @@ static LineParams line_params(const zm_plan_s *p, int kind, const void *in, void
     return lp;
 }
 
+// The out-of-place forward configuration of a 2D plan (x pass in -> work, y pass
+// work -> out, each pass with its own tile shape and a wider row interleave; the
+// in-place y pass rules out interleaves wider than its tile), or false.
+static bool fwd_oop_config(const zm_plan_s *p, int *vx, int *vy, int *lg) {
+    if (p->g.dim != 2 || (p->flags & ZM_FLAG_PERMUTE_ONLY) || p->nvariants == 0 || p->variant != 0) return false;
+    const int ok = p->dtype == ZM_C128 ? zm::fused_fwd_oop_c128(p->g.logVEC, p->g.logM, vx, vy, lg)
+                                       : zm::fused_fwd_oop_c64(p->g.logVEC, p->g.logM, vx, vy, lg);
+    if (!ok) return false;
+    if (*lg > p->g.logVP) *lg = p->g.logVP;
+    return true;
+}
+
+// `variant` / `lg` >= 0 override the plan's tile shape and row interleave for this pass.
 static int run_pass(const zm_plan_s *p, int kind, bool inv, const void *in, void *out, bool scale,
-                    double sre, double sim, cudaStream_t st) {
+                    double sre, double sim, cudaStream_t st, int variant = -1, int lg = -1) {
     LineParams lp = line_params(p, kind, in, out);
+    if (variant >= 0) lp.variant = variant;
+    if (lg >= 0) lp.lg_inter = lg;
     if (scale) {
         lp.apply_scale = 1;
         lp.scale_re = sre;
@@ -204,6 +219,14 @@ static int forward_impl(zm_plan p, const void *in, void *out, void *work, bool s
     if (!fft_supported(p, &why)) return fail(ZM_ERR_UNSUPPORTED, "%s", why.c_str());
     if (work && (!aligned16(work))) return fail(ZM_ERR_MISALIGNED, "work is not 16-byte aligned");
     if (p->g.dim == 2) {
+        int vx, vy, lg;
+        if (work && fwd_oop_config(p, &vx, &vy, &lg)) {
+            if (overlap(work, in, F) || overlap(work, out, F))
+                return fail(ZM_ERR_INVALID_ARG, "work overlaps in/out");
+            // x pass in -> work, y pass work -> out (no in-place constraint on the tile)
+            if ((rc = run_pass(p, zm::PASS_X2, false, in, work, false, 0, 0, st, vx, lg))) return rc;
+            return run_pass(p, zm::PASS_Y2, false, work, out, scale, sre, sim, st, vy, lg);
+        }
         // x pass: real layout -> REPACK layout (in -> out); y pass in place on out
         if ((rc = run_pass(p, zm::PASS_X2, false, in, out, false, 0, 0, st))) return rc;
         return run_pass(p, zm::PASS_Y2, false, out, out, scale, sre, sim, st);

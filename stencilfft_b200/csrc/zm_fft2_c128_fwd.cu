@@ -56,4 +56,10 @@ int fused_interleave_lg_c128(int logvec, int logm, int variant) {
     }
 }
 
+int fused_fwd_oop_c128(int logvec, int logm, int *vx, int *vy, int *lg) {
+    switch ((logvec << 8) | logm) {
+    default: return 0;
+    }
+}
+
 }  // namespace zm

@@ -73,4 +73,11 @@ int fused_interleave_lg_c64(int logvec, int logm, int variant) {
     }
 }
 
+int fused_fwd_oop_c64(int logvec, int logm, int *vx, int *vy, int *lg) {
+    switch ((logvec << 8) | logm) {
+    case (6 << 8) | 8: *vx = 2; *vy = 2; *lg = 3; return 1;
+    default: return 0;
+    }
+}
+
 }  // namespace zm
