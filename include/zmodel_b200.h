@@ -183,8 +183,8 @@ int zm_fft_inverse_static(zm_plan plan, const void *in, void *out, double scale_
  * has no 1/h^2 factor: inv_h2 = 1 reproduces it.
  * zm_dx / zm_dy replace dx / dy (dx.cu:10-82, dy.cu:10-103), the 4th-order
  * central differences (f[i-2] - 8 f[i-1] + 8 f[i+1] - f[i+2]) / (12 delta) along
- * x (columns) / y (rows) of a 2D field, applied to each complex component.  They
- * need B >= 2 like the reference (dx.cu:100, dy.cu:123).
+ * x (columns) / y (rows) of a 2D field, applied to each complex component.  The
+ * reference needs B >= 2 (dx.cu:100, dy.cu:123); these also accept B = 1.
  * zm_dx_real / zm_dy_real take a real field (double for ZM_C128 plans, float for
  * ZM_C64), the reference's Scalar form.
  */
@@ -193,6 +193,12 @@ int zm_dx(zm_plan plan, const void *in, void *out, double delta, void *stream);
 int zm_dy(zm_plan plan, const void *in, void *out, double delta, void *stream);
 int zm_dx_real(zm_plan plan, const void *in, void *out, double delta, void *stream);
 int zm_dy_real(zm_plan plan, const void *in, void *out, double delta, void *stream);
+/* The 2D Laplacian, dx and dy of one complex field in one launch (no reference
+ * counterpart: the reference runs three kernels with three halo exchanges).  Each output
+ * is bit-identical to zm_laplace(inv_h2) / zm_dx(delta) / zm_dy(delta); the field is read
+ * once (4 field transfers instead of 6).  The four buffers must not overlap. */
+int zm_laplace_dx_dy(zm_plan plan, const void *in, void *lap, void *dx, void *dy, double inv_h2,
+                     double delta, void *stream);
 
 /*
  * Vector-Jacobian products (no counterpart in the reference).  Gradients use the

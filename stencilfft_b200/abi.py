@@ -71,6 +71,7 @@ SIGNATURES = {
     "zm_fft_inverse": [_P, _P, _P, _P, _D, _D, _P],
     "zm_fft_inverse_static": [_P, _P, _P, _D, _D, _P],
     "zm_laplace": [_P, _P, _P, _D, _P],
+    "zm_laplace_dx_dy": [_P, _P, _P, _P, _P, _D, _D, _P],
     "zm_dx": [_P, _P, _P, _D, _P],
     "zm_dy": [_P, _P, _P, _D, _P],
     "zm_dx_real": [_P, _P, _P, _D, _P],

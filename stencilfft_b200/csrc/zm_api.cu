@@ -556,6 +556,25 @@ static int stencil_call(zm_plan plan, int op, bool real_field, const void *in, v
     return ZM_OK;
 }
 
+int zm_laplace_dx_dy(zm_plan plan, const void *in, void *lap, void *dx, void *dy, double inv_h2,
+                     double delta, void *stream) {
+    int rc;
+    if ((rc = check_device_plan(plan))) return rc;
+    if ((rc = check_field(plan, in, "in")) || (rc = check_field(plan, lap, "lap")) ||
+        (rc = check_field(plan, dx, "dx")) || (rc = check_field(plan, dy, "dy")))
+        return rc;
+    if (plan->g.dim != 2) return fail(ZM_ERR_UNSUPPORTED, "dx / dy are defined on 2D plans only");
+    if (delta == 0.0) return fail(ZM_ERR_INVALID_ARG, "delta must be non-zero");
+    const size_t F = plan->total * plan->elem_bytes;
+    const void *bufs[4] = {in, lap, dx, dy};
+    for (int a = 0; a < 4; a++)
+        for (int b = a + 1; b < 4; b++)
+            if (overlap(bufs[a], bufs[b], F)) return fail(ZM_ERR_INVALID_ARG, "in, lap, dx and dy must not overlap");
+    cudaError_t e = zm::launch_stencil(plan, zm::ST_ALL, false, in, lap, inv_h2, as_stream(stream), dx, dy, delta);
+    if (e != cudaSuccess) return cuda_fail(e, "stencil launch");
+    return ZM_OK;
+}
+
 int zm_laplace(zm_plan plan, const void *in, void *out, double inv_h2, void *stream) {
     return stencil_call(plan, zm::ST_LAPLACE, false, in, out, inv_h2, stream);
 }

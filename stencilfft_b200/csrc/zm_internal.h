@@ -38,9 +38,11 @@ int fused_fwd_oop_c64(int logvec, int logm, int *vx, int *vy, int *lg);
 int fused_fwd_oop_c128(int logvec, int logm, int *vx, int *vy, int *lg);
 
 // zm_stencil.cu
-enum StencilOp : int { ST_LAPLACE = 0, ST_DX = 1, ST_DY = 2 };
+enum StencilOp : int { ST_LAPLACE = 0, ST_DX = 1, ST_DY = 2, ST_ALL = 3 };
+// ST_ALL (2D): Laplacian (coef) into out, dx / dy (coef2 = delta) into out2 / out3
 cudaError_t launch_stencil(const zm_plan_s *p, int op, bool real_field, const void *in, void *out,
-                           double coef, cudaStream_t st);
+                           double coef, cudaStream_t st, void *out2 = nullptr, void *out3 = nullptr,
+                           double coef2 = 1.0);
 
 // zm_layout.cu
 cudaError_t launch_convert(const zm_plan_s *p, bool reciprocal, bool to_natural, const void *in,

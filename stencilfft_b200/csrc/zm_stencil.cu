@@ -65,9 +65,13 @@ template <typename S> struct vec16 {
 
 // S = scalar type; NC = scalars per element (2 complex, 1 real).  One thread = one
 // 16-byte vector = K = 16 / (NC * sizeof(S)) consecutive elements.
+// OP = ST_ALL (2D): the Laplacian (coef) into `out`, dx and dy (coef2 = delta) into
+// `out2` / `out3` from one read of the neighbourhood; each result is computed exactly as
+// by its own kernel.
 template <typename S, int NC, int OP, int DIM>
 __global__ void __launch_bounds__(256) stencil_kernel(const S *__restrict__ in, S *__restrict__ out,
-                                                      const Geom g, int64_t nvec, S coef) {
+                                                      S *__restrict__ out2, S *__restrict__ out3,
+                                                      const Geom g, int64_t nvec, S coef, S coef2) {
     using O = ops<S>;
     using V = vec16<S>;
     constexpr int K = V::n / NC;                 // elements per vector
@@ -151,7 +155,34 @@ __global__ void __launch_bounds__(256) stencil_kernel(const S *__restrict__ in, 
         return r;
     };
     V res;
-    if (OP == ST_LAPLACE) {
+    if (OP == ST_ALL) {
+        const V up = as(vrow(-1)), dn = as(vrow(1)), lf = vcol(-1), rt = vcol(1);
+        const V up2 = as(vrow(-2)), dn2 = as(vrow(2)), lf2 = vcol(-2), rt2 = vcol(2);
+        const V c = as(__ldg(reinterpret_cast<const uint4 *>(in + e * NC)));
+        V rx, ry;
+        const S den = O::mul((S)12, coef2);
+#pragma unroll
+        for (int i = 0; i < V::n; i++) {
+            S s = O::add((S)0, up.v[i]);
+            s = O::add(s, dn.v[i]);
+            s = O::add(s, lf.v[i]);
+            s = O::add(s, rt.v[i]);
+            s = O::fmaop((S)(-4), c.v[i], s);
+            res.v[i] = O::mul(s, coef);
+            S x = O::add((S)0, O::mul(lf.v[i], (S)-8));
+            x = O::add(x, lf2.v[i]);
+            x = O::add(x, O::mul(rt.v[i], (S)8));
+            x = O::sub(x, rt2.v[i]);
+            rx.v[i] = O::div(x, den);
+            S y = O::add((S)0, O::mul(up.v[i], (S)-8));
+            y = O::add(y, up2.v[i]);
+            y = O::add(y, O::mul(dn.v[i], (S)8));
+            y = O::sub(y, dn2.v[i]);
+            ry.v[i] = O::div(y, den);
+        }
+        *reinterpret_cast<uint4 *>(out2 + e * NC) = *reinterpret_cast<const uint4 *>(&rx);
+        *reinterpret_cast<uint4 *>(out3 + e * NC) = *reinterpret_cast<const uint4 *>(&ry);
+    } else if (OP == ST_LAPLACE) {
         // laplace.cu:91-168 / laplace3d.cu:98-224 accumulation order
         const V up = as(vrow(-1)), dn = as(vrow(1)), lf = vcol(-1), rt = vcol(1);
         const V c = as(__ldg(reinterpret_cast<const uint4 *>(in + e * NC)));
@@ -195,36 +226,41 @@ __global__ void __launch_bounds__(256) stencil_kernel(const S *__restrict__ in, 
 }
 
 template <typename S, int NC>
-static cudaError_t launch_s(const zm_plan_s *p, int op, const void *in, void *out, double coef,
-                            cudaStream_t st) {
+static cudaError_t launch_s(const zm_plan_s *p, int op, const void *in, void *out, void *out2, void *out3,
+                            double coef, double coef2, cudaStream_t st) {
     constexpr int K = 16 / (int)sizeof(S) / NC;
     if (p->g.L % K) return cudaErrorInvalidValue;
     const int64_t nvec = p->total / K;
     const int threads = 256;
     const unsigned grid = (unsigned)((nvec + threads - 1) / threads);
     const S *i = reinterpret_cast<const S *>(in);
-    S *o = reinterpret_cast<S *>(out);
-    const S c = (S)coef;
+    S *o = reinterpret_cast<S *>(out), *o2 = reinterpret_cast<S *>(out2), *o3 = reinterpret_cast<S *>(out3);
+    const S c = (S)coef, c2 = (S)coef2;
     if (p->g.dim == 2) {
-        if (op == ST_LAPLACE) stencil_kernel<S, NC, ST_LAPLACE, 2><<<grid, threads, 0, st>>>(i, o, p->g, nvec, c);
-        else if (op == ST_DX) stencil_kernel<S, NC, ST_DX, 2><<<grid, threads, 0, st>>>(i, o, p->g, nvec, c);
-        else stencil_kernel<S, NC, ST_DY, 2><<<grid, threads, 0, st>>>(i, o, p->g, nvec, c);
+        if (op == ST_LAPLACE)
+            stencil_kernel<S, NC, ST_LAPLACE, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2);
+        else if (op == ST_DX)
+            stencil_kernel<S, NC, ST_DX, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2);
+        else if (op == ST_DY)
+            stencil_kernel<S, NC, ST_DY, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2);
+        else
+            stencil_kernel<S, NC, ST_ALL, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2);
     } else {
         if (op != ST_LAPLACE) return cudaErrorInvalidValue;
-        stencil_kernel<S, NC, ST_LAPLACE, 3><<<grid, threads, 0, st>>>(i, o, p->g, nvec, c);
+        stencil_kernel<S, NC, ST_LAPLACE, 3><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2);
     }
     count_launch();
     return cudaGetLastError();
 }
 
 cudaError_t launch_stencil(const zm_plan_s *p, int op, bool real_field, const void *in, void *out,
-                           double coef, cudaStream_t st) {
+                           double coef, cudaStream_t st, void *out2, void *out3, double coef2) {
     if (p->dtype == 0) {
-        return real_field ? launch_s<double, 1>(p, op, in, out, coef, st)
-                          : launch_s<double, 2>(p, op, in, out, coef, st);
+        return real_field ? launch_s<double, 1>(p, op, in, out, out2, out3, coef, coef2, st)
+                          : launch_s<double, 2>(p, op, in, out, out2, out3, coef, coef2, st);
     }
-    return real_field ? launch_s<float, 1>(p, op, in, out, coef, st)
-                      : launch_s<float, 2>(p, op, in, out, coef, st);
+    return real_field ? launch_s<float, 1>(p, op, in, out, out2, out3, coef, coef2, st)
+                      : launch_s<float, 2>(p, op, in, out, out2, out3, coef, coef2, st);
 }
 
 }  // namespace zm

@@ -152,6 +152,15 @@ class Plan:
 
     laplace_3d = laplace
 
+    def laplace_dx_dy(self, inp, lap, gx, gy, inv_h2: float = 1.0, delta: float = 1.0, stream=None):
+        """Laplacian, dx and dy of a 2D complex field in one launch (each bit-identical to
+        laplace / dx / dy)."""
+        for t, nm in ((inp, "in"), (lap, "lap"), (gx, "dx"), (gy, "dy")):
+            self._check(t, nm)
+        check(lib().zm_laplace_dx_dy(self._h, _ptr(inp), _ptr(lap), _ptr(gx), _ptr(gy), float(inv_h2),
+                                     float(delta), _stream_ptr(stream)), "zm_laplace_dx_dy")
+        return lap, gx, gy
+
     def dx(self, inp, out, delta: float = 1.0, stream=None):
         real = not inp.is_complex()
         self._check(inp, "in", real), self._check(out, "out", real)

@@ -166,3 +166,23 @@ def test_dx_dy_accept_b1_as_extension():
     gx = O.real_layout_to_natural(to_host(d1), 2, n, b, p)
     rx = (np.roll(x, 2, 1) - 8 * np.roll(x, 1, 1) + 8 * np.roll(x, -1, 1) - np.roll(x, -2, 1)) / 12
     assert relerr(gx, rx) < 1e-14
+
+
+@pytest.mark.parametrize("dt", ["c128", "c64"])
+@pytest.mark.parametrize("n,b,p", [(64, 4, 2), (64, 1, 2), (256, 16, 4), (1024, 32, 2), (512, 8, 4)])
+def test_laplace_dx_dy_fused_bit_identical(n, b, p, dt):
+    """zm_laplace_dx_dy: each output bit-identical to its own stencil call."""
+    import torch
+    from stencilfft_b200 import abi
+    pl = _plan(2, n, b, p, dt)
+    u = pl.empty()
+    pl.fill(u, abi.ZM_FIELD_GAUSSIAN, 5)
+    lap, gx, gy = pl.empty(), pl.empty(), pl.empty()
+    pl.laplace_dx_dy(u, lap, gx, gy, inv_h2=float(n * n), delta=1.0 / n)
+    ref = pl.empty()
+    pl.laplace(u, ref, inv_h2=float(n * n))
+    assert torch.equal(lap, ref)
+    pl.dx(u, ref, delta=1.0 / n)
+    assert torch.equal(gx, ref)
+    pl.dy(u, ref, delta=1.0 / n)
+    assert torch.equal(gy, ref)
