@@ -17,7 +17,8 @@
 //     butterfly sits at a compile-time offset from its base;
 //   * each sub-transform is at most two register stages of radix <= 16 (Stockham
 //     indexing), with the stage twiddles w_VEC, w_M in shared memory and the inter-step
-//     twiddle w_N^{n1 k2} from an FP64 power walk;
+//     twiddle w_N^{n1 k2} from two shared-memory factor tables (complex64 with one CTA
+//     per tile: two compensated products) or an FP64 power walk;
 //   * one tile per cluster, the vector side moved through registers / 16-byte vectors;
 //     or, for forward passes with two row stages in the persistent variants (PERS), a
 //     cluster walks tiles c, c + clusters, ... and each CTA fetches the vector-side rows
@@ -110,6 +111,14 @@ template <int LV, int LM, int CL, int TL, int NT> struct SliceGeom {
     // (lanes over sg lines x RA2 points, then rows) free of bank conflicts
     static constexpr int SR(int sg) { return sg * VEC + (sg * RA2) % 16; }
     static constexpr int stage_elems(int sg) { return sg > TL ? 0 : (TL / sg) * ML * SR(sg); }
+    // complex64 inter-step twiddles w_N^m = w_N^{(m >> TLO) 2^TLO} w_N^{m mod 2^TLO}:
+    // two tables of NTA and NTB entries (hi/lo pairs) in shared memory.  Used by the
+    // one-CTA-per-tile shapes; with a cluster the exchange through distributed shared
+    // memory already saturates the shared-memory pipe, and the FP64 walk (FP64 and
+    // conversion pipes) is faster there.
+    static constexpr int LOGN = LV + LM, TLO = LOGN / 2;
+    static constexpr int NTA = 1 << (LOGN - TLO), NTB = 1 << TLO;
+    template <typename T> static constexpr bool twtab() { return sizeof(T) == 4 && CL == 1; }
     static constexpr int smax(int a, int b) { return a > b ? a : b; }
     static constexpr int STAGE_ELEMS = smax(stage_elems(1), smax(stage_elems(2), stage_elems(4)));
 };
@@ -118,10 +127,15 @@ template <typename T, int LV, int LM, int CL, int TL, int NT>
 constexpr size_t fused_tables_offset() {
     return sizeof(cpx<T>) * (size_t)SliceGeom<LV, LM, CL, TL, NT>::ELEMS;
 }
+// twiddle tables: w_VEC, w_M and, for complex64, the two inter-step tables
+template <typename T, int LV, int LM, int CL, int TL, int NT>
+constexpr size_t fused_twiddle_entries() {
+    using SG = SliceGeom<LV, LM, CL, TL, NT>;
+    return ((size_t)1 << LV) + ((size_t)1 << LM) + (SG::template twtab<T>() ? (size_t)(SG::NTA + SG::NTB) : 0);
+}
 template <typename T, int LV, int LM, int CL, int TL, int NT>
 constexpr size_t fused_stage_offset() {
-    return fused_tables_offset<T, LV, LM, CL, TL, NT>() +
-           sizeof(tw<T>) * (((size_t)1 << LV) + ((size_t)1 << LM));
+    return fused_tables_offset<T, LV, LM, CL, TL, NT>() + sizeof(tw<T>) * fused_twiddle_entries<T, LV, LM, CL, TL, NT>();
 }
 
 // Forward passes with two row stages can run persistent with a staging buffer (PERS,
@@ -172,6 +186,8 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
     C *S = reinterpret_cast<C *>(smem_raw);
     Wt *stv = reinterpret_cast<Wt *>(smem_raw + fused_tables_offset<T, LV, LM, CL, TL, NT>());  // w_VEC^m
     Wt *stm = stv + VEC;                                                                          // w_M^m
+    Wt *sta = stm + M;                     // complex64: w_N^{a 2^TLO}, a < NTA
+    Wt *stb = sta + SG::NTA;               // complex64: w_N^b, b < NTB
     __shared__ int64_t s_abase[TL], s_fbase[TL];
     __shared__ uint64_t s_bar;
 
@@ -188,6 +204,11 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
         const Wt *tv = reinterpret_cast<const Wt *>(prm.twv);
         const Wt *tm = reinterpret_cast<const Wt *>(prm.twm);
         for (int i = tid; i < VEC + M; i += NT) stv[i] = i < VEC ? ldtw(tv, i) : ldtw(tm, i - VEC);
+        if constexpr (SG::template twtab<T>()) {
+            const double2 *td = reinterpret_cast<const double2 *>(prm.twd);
+            for (int i = tid; i < SG::NTA + SG::NTB; i += NT)
+                sta[i] = tw_from_d<T>(ldd2(td + (i < SG::NTA ? (i << SG::TLO) : i - SG::NTA)));
+        }
     }
     // per-line bases of the tile starting at line l0 (the caller synchronises)
     auto set_tile = [&](int64_t l0) {
@@ -264,18 +285,44 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
             t = rr / nj;
         }
     };
-    // inter-step twiddles w_N^{(j + s r) k2}, r = 0, 1, ...: FP64 power walk from the
-    // table w_N^m (m < 16 VEC), then the stored form (hi/lo split for complex64)
+    // inter-step twiddles w_N^{(j + s r) k2}, r = 0, 1, ... applied to a point:
+    //   complex128: FP64 power walk from the table w_N^m (m < 16 VEC);
+    //   complex64, one CTA per tile: exponent m = (j + s r) k2 mod N stepped in integers
+    //               and the point multiplied by the two shared-memory factors of w_N^m,
+    //               each a compensated hi/lo product (no FP64 work or conversions);
+    //   complex64 with a cluster: the FP64 walk, each twiddle split into hi/lo
     const double2 *Td = reinterpret_cast<const double2 *>(prm.twd);
     struct Walk {
-        double2 w, step;
-        ZM_DEV tw<T> next() {
-            const tw<T> r = tw_from_d<T>(w);
-            w = cmul_d(w, step);
-            return r;
+        double2 w, step;   // complex128
+        int m, dm;         // complex64
+        const Wt *ta, *tb;
+        ZM_DEV C apply(C x, bool conj) {   // conj: multiply by conj(w) (a constant at every call)
+            if constexpr (SG::template twtab<T>()) {
+                const Wt a = ta[m >> SG::TLO], b = tb[m & (SG::NTB - 1)];
+                x = conj ? twmul<true>(twmul<true>(x, a), b) : twmul<false>(twmul<false>(x, a), b);
+                m = (m + dm) & (SG::N - 1);
+                return x;
+            } else {
+                const Wt t = tw_from_d<T>(w);
+                const C r = conj ? twmul<true>(x, t) : twmul<false>(x, t);
+                w = cmul_d(w, step);
+                return r;
+            }
         }
     };
-    auto walk = [&](int j, int s, int k2) { return Walk{ldd2(Td + j * k2), ldd2(Td + s * k2)}; };
+    auto walk = [&](int j, int s, int k2) {
+        Walk wk;
+        if constexpr (SG::template twtab<T>()) {
+            wk.m = (j * k2) & (SG::N - 1);
+            wk.dm = (s * k2) & (SG::N - 1);
+            wk.ta = sta;
+            wk.tb = stb;
+        } else {
+            wk.w = ldd2(Td + j * k2);
+            wk.step = ldd2(Td + s * k2);
+        }
+        return wk;
+    };
     auto xidx_of_e = [](int e) {
         const int t = e / (ML * VEC), r = e % (ML * VEC);
         return SG::X(t, r >> LV, r & (VEC - 1));
@@ -344,7 +391,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
             Walk wk = walk(zj[i], RC2, k2_0 + zk[i]);               // n1 = zj + RC2 * r
 #pragma unroll
             for (int r = 0; r < RC1; r++)
-                z[i][r] = twmul<false>(S[SG::Y(zt[i], zk[i], zj[i] + RC2 * r)], wk.next());
+                z[i][r] = wk.apply(S[SG::Y(zt[i], zk[i], zj[i] + RC2 * r)], false);
         }
 #pragma unroll
         for (int i = 0; i < NU; i++) dft<RC1, DIR, T>(z[i]);
@@ -539,7 +586,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
                     Walk wk = walk(0, 1, k2);                            // n1 = r
 #pragma unroll
                     for (int r = 0; r < RC1; r++)
-                        xowner(r)[SG::X(zt[i], r % ML, k2)] = twmul<true>(z[i][r], wk.next());
+                        xowner(r)[SG::X(zt[i], r % ML, k2)] = wk.apply(z[i][r], true);
                 }
             } else {
 #pragma unroll
@@ -574,7 +621,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
 #pragma unroll
                     for (int r = 0; r < RC2; r++) {
                         const int n1 = yj[i] + RC1 * r;
-                        xowner(n1)[SG::X(yt[i], n1 % ML, k2)] = twmul<true>(y[i][r], wk.next());
+                        xowner(n1)[SG::X(yt[i], n1 % ML, k2)] = wk.apply(y[i][r], true);
                     }
                 }
             }
