@@ -151,7 +151,6 @@ static LineParams line_params(const zm_plan_s *p, int kind, const void *in, void
     lp.in = in;
     lp.out = out;
     lp.twN = p->twN;
-    lp.W = p->W;
     lp.twd = p->twd;
     lp.twv = p->twv;
     lp.twm = p->twm;
@@ -315,7 +314,7 @@ int zm_plan_create(zm_plan *plan, int dim, int64_t n, int64_t b, int64_t p, int 
     // Also, for the size-specialised passes: w_N^m in FP64 for every dtype (the
     // inter-step twiddles are generated from it on the device) and the sub-transform
     // tables w_VEC^m, w_M^m.  All four tables share one allocation of 16-byte entries.
-    P->twN = P->W = P->twv = P->twm = P->twd = nullptr;
+    P->twN = P->twv = P->twm = P->twd = nullptr;
     P->dev_err = nullptr;
     if (flags & ZM_FLAG_HOST_ONLY) {
         *plan = P;

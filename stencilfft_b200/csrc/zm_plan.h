@@ -32,7 +32,6 @@ struct LineParams {
     const void *in;
     void *out;
     const void *twN;   // w_N^m, m < N, forward sign (tw<double> or tw<float>)
-    const void *W;     // w_N^{n1 k2} in [n1][k2] order (N entries)
     const void *twv;   // w_VEC^m, m < VEC
     const void *twm;   // w_M^m, m < M
     const void *twd;   // w_N^m, m < N, in FP64 (double2) for every dtype
@@ -57,7 +56,6 @@ struct zm_plan_s {
     size_t elem_bytes;
     int device;
     void *twN;        // device twiddle table (N entries)
-    void *W;          // w_N^{n1 k2}, [n1][k2] order (N entries)
     void *twv;        // w_VEC^m (VEC entries)
     void *twm;        // w_M^m (M entries)
     void *twd;        // w_N^m in FP64 (N entries; the same table as twN for complex128)

@@ -239,3 +239,31 @@ def test_autotune_b_picks_a_valid_layout():
     out = pl.empty()
     pl.forward_fft(to_dev(x, "c64"), out, work=pl.empty())
     assert relerr(to_host(out), O.forward_fft(x, 2, n, b, p)) < TOL["c64"]
+
+
+def test_error_paths_fused_stencils_and_workspace():
+    """Argument checks of zm_laplace_dx_dy and of the workspace of the out-of-place
+    forward configuration; the context stays usable."""
+    import torch
+    from stencilfft_b200 import ZmError, abi
+    pl = _plan(2, 256, 16, 4, "c64")
+    a, b_, c, d = pl.empty(), pl.empty(), pl.empty(), pl.empty()
+    pl.fill(a, abi.ZM_FIELD_GAUSSIAN, 1)
+    with pytest.raises(ZmError):
+        pl.laplace_dx_dy(a, b_, b_, c)                 # outputs overlap
+    with pytest.raises(ZmError):
+        pl.laplace_dx_dy(a, a, c, d)                   # in overlaps an output
+    with pytest.raises(ZmError):
+        pl.laplace_dx_dy(a, b_, c, d, delta=0.0)
+    p3 = _plan(3, 16, 2, 2, "c64")
+    x = p3.empty()
+    with pytest.raises(ZmError):
+        p3.laplace_dx_dy(x, p3.empty(), p3.empty(), p3.empty())
+    big = _plan(2, 16384, 64, 4, "c64")                # has the out-of-place forward configuration
+    L = abi.lib()
+    u = big.empty()
+    o = big.empty()
+    # a workspace that overlaps the output is rejected before any launch
+    assert L.zm_fft_forward(big.handle, u.data_ptr(), o.data_ptr(), o.data_ptr(), None) == abi.ZM_ERR_INVALID_ARG
+    del u, o
+    torch.cuda.synchronize()
