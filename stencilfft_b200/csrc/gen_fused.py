@@ -7,7 +7,7 @@ re-measures them for a plan."""
 VARIANTS = {
     "c64": {
         (4, 4): [(1, 32, 512)], (4, 5): [(1, 16, 512)], (4, 6): [(1, 8, 512), (1, 4, 256)],
-        (2, 7): [(1, 16, 512)], (5, 6): [(1, 4, 512)],
+        (2, 7): [(1, 8, 256), (1, 16, 512), (1, 32, 1024), (1, 4, 128)], (5, 6): [(1, 4, 512)],
         (5, 7): [(1, 2, 512), (2, 2, 256), (2, 4, 512)],
         (4, 8): [(1, 2, 512), (2, 4, 512)],
         (5, 8): [(2, 2, 512), (1, 1, 512), (2, 1, 256), (4, 4, 512), (2, 4, 1024)],
@@ -15,7 +15,7 @@ VARIANTS = {
         (6, 8): [(4, 2, 512), (2, 1, 512), (1, 1, 1024), (8, 4, 512), (4, 4, 1024), (4, 2, 512, "p")],
     },
     "c128": {
-        (4, 4): [(1, 16, 256)], (4, 5): [(1, 8, 256)], (4, 6): [(1, 4, 256)], (2, 7): [(1, 8, 256)],
+        (4, 4): [(1, 16, 256)], (4, 5): [(1, 8, 256)], (4, 6): [(1, 4, 256)], (2, 7): [(1, 8, 256), (1, 4, 128), (1, 16, 512)],
         (5, 6): [(1, 2, 256)], (5, 7): [(1, 1, 256), (2, 2, 256)], (4, 8): [(1, 1, 256), (2, 2, 256)],
         (5, 8): [(1, 1, 512), (2, 1, 256)], (6, 7): [(2, 1, 256), (1, 1, 512)],
         (6, 8): [(2, 1, 512), (4, 1, 256), (4, 2, 512)],

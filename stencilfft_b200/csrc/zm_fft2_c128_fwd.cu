@@ -13,6 +13,8 @@ cudaError_t launch_fused_c128_fwd(const LineParams &prm, cudaStream_t st, bool *
     case (4 << 16) | (5 << 8) | 0: return launch_fused<double, 4, 5, 1, 8, 256, false, false>(prm, st);
     case (4 << 16) | (6 << 8) | 0: return launch_fused<double, 4, 6, 1, 4, 256, false, false>(prm, st);
     case (2 << 16) | (7 << 8) | 0: return launch_fused<double, 2, 7, 1, 8, 256, false, false>(prm, st);
+    case (2 << 16) | (7 << 8) | 1: return launch_fused<double, 2, 7, 1, 4, 128, false, false>(prm, st);
+    case (2 << 16) | (7 << 8) | 2: return launch_fused<double, 2, 7, 1, 16, 512, false, false>(prm, st);
     case (5 << 16) | (6 << 8) | 0: return launch_fused<double, 5, 6, 1, 2, 256, false, false>(prm, st);
     case (5 << 16) | (7 << 8) | 0: return launch_fused<double, 5, 7, 1, 1, 256, false, false>(prm, st);
     case (5 << 16) | (7 << 8) | 1: return launch_fused<double, 5, 7, 2, 2, 256, false, false>(prm, st);
@@ -36,7 +38,7 @@ int fused_variants_c128(int logvec, int logm) {
     case (4 << 8) | 4: return 1;
     case (4 << 8) | 5: return 1;
     case (4 << 8) | 6: return 1;
-    case (2 << 8) | 7: return 1;
+    case (2 << 8) | 7: return 3;
     case (5 << 8) | 6: return 1;
     case (5 << 8) | 7: return 2;
     case (4 << 8) | 8: return 2;

@@ -13,6 +13,8 @@ cudaError_t launch_fused_c128_inv(const LineParams &prm, cudaStream_t st, bool *
     case (4 << 16) | (5 << 8) | 0: return launch_fused<double, 4, 5, 1, 8, 256, true, false>(prm, st);
     case (4 << 16) | (6 << 8) | 0: return launch_fused<double, 4, 6, 1, 4, 256, true, false>(prm, st);
     case (2 << 16) | (7 << 8) | 0: return launch_fused<double, 2, 7, 1, 8, 256, true, false>(prm, st);
+    case (2 << 16) | (7 << 8) | 1: return launch_fused<double, 2, 7, 1, 4, 128, true, false>(prm, st);
+    case (2 << 16) | (7 << 8) | 2: return launch_fused<double, 2, 7, 1, 16, 512, true, false>(prm, st);
     case (5 << 16) | (6 << 8) | 0: return launch_fused<double, 5, 6, 1, 2, 256, true, false>(prm, st);
     case (5 << 16) | (7 << 8) | 0: return launch_fused<double, 5, 7, 1, 1, 256, true, false>(prm, st);
     case (5 << 16) | (7 << 8) | 1: return launch_fused<double, 5, 7, 2, 2, 256, true, false>(prm, st);

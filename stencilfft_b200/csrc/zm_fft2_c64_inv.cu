@@ -13,7 +13,10 @@ cudaError_t launch_fused_c64_inv(const LineParams &prm, cudaStream_t st, bool *h
     case (4 << 16) | (5 << 8) | 0: return launch_fused<float, 4, 5, 1, 16, 512, true, false>(prm, st);
     case (4 << 16) | (6 << 8) | 0: return launch_fused<float, 4, 6, 1, 8, 512, true, false>(prm, st);
     case (4 << 16) | (6 << 8) | 1: return launch_fused<float, 4, 6, 1, 4, 256, true, false>(prm, st);
-    case (2 << 16) | (7 << 8) | 0: return launch_fused<float, 2, 7, 1, 16, 512, true, false>(prm, st);
+    case (2 << 16) | (7 << 8) | 0: return launch_fused<float, 2, 7, 1, 8, 256, true, false>(prm, st);
+    case (2 << 16) | (7 << 8) | 1: return launch_fused<float, 2, 7, 1, 16, 512, true, false>(prm, st);
+    case (2 << 16) | (7 << 8) | 2: return launch_fused<float, 2, 7, 1, 32, 1024, true, false>(prm, st);
+    case (2 << 16) | (7 << 8) | 3: return launch_fused<float, 2, 7, 1, 4, 128, true, false>(prm, st);
     case (5 << 16) | (6 << 8) | 0: return launch_fused<float, 5, 6, 1, 4, 512, true, false>(prm, st);
     case (5 << 16) | (7 << 8) | 0: return launch_fused<float, 5, 7, 1, 2, 512, true, false>(prm, st);
     case (5 << 16) | (7 << 8) | 1: return launch_fused<float, 5, 7, 2, 2, 256, true, false>(prm, st);
