@@ -8,10 +8,10 @@ VARIANTS = {
     "c64": {
         (4, 4): [(1, 32, 512)], (4, 5): [(1, 16, 512)], (4, 6): [(1, 8, 512), (1, 4, 256)],
         (2, 7): [(1, 8, 256), (1, 16, 512), (1, 32, 1024), (1, 4, 128)], (5, 6): [(1, 4, 512)],
-        (5, 7): [(1, 2, 512), (2, 2, 256), (2, 4, 512)],
-        (4, 8): [(1, 2, 512), (2, 4, 512)],
-        (5, 8): [(2, 2, 512), (1, 1, 512), (2, 1, 256), (4, 4, 512), (2, 4, 1024)],
-        (6, 7): [(1, 1, 512), (2, 2, 512)],
+        (5, 7): [(1, 2, 512), (2, 2, 256), (2, 4, 512), (1, 1, 256), (1, 4, 1024)],
+        (4, 8): [(1, 2, 512), (2, 4, 512), (1, 1, 256), (1, 4, 1024)],
+        (5, 8): [(2, 2, 512), (1, 1, 512), (2, 1, 256), (4, 4, 512), (2, 4, 1024), (1, 2, 1024)],
+        (6, 7): [(2, 2, 512), (1, 1, 512), (1, 2, 1024)],
         (6, 8): [(4, 2, 512), (2, 1, 512), (1, 1, 1024), (8, 4, 512), (4, 4, 1024), (4, 2, 512, "p")],
     },
     "c128": {
@@ -27,7 +27,7 @@ VARIANTS = {
 # one 1024-thread CTA per line in both passes with 8-row interleave, 3.73 ms per forward
 # transform against 4.61 for the in-place default.
 FWD_OOP = {
-    "c64": {(6, 8): (2, 2, 3)},
+    "c64": {(6, 8): (2, 2, 3), (5, 8): (5, 5, 1), (6, 7): (2, 2, 1)},
     "c128": {},
 }
 T = {"c64": "float", "c128": "double"}

@@ -21,15 +21,21 @@ cudaError_t launch_fused_c64_fwd(const LineParams &prm, cudaStream_t st, bool *h
     case (5 << 16) | (7 << 8) | 0: return launch_fused<float, 5, 7, 1, 2, 512, false, false>(prm, st);
     case (5 << 16) | (7 << 8) | 1: return launch_fused<float, 5, 7, 2, 2, 256, false, false>(prm, st);
     case (5 << 16) | (7 << 8) | 2: return launch_fused<float, 5, 7, 2, 4, 512, false, false>(prm, st);
+    case (5 << 16) | (7 << 8) | 3: return launch_fused<float, 5, 7, 1, 1, 256, false, false>(prm, st);
+    case (5 << 16) | (7 << 8) | 4: return launch_fused<float, 5, 7, 1, 4, 1024, false, false>(prm, st);
     case (4 << 16) | (8 << 8) | 0: return launch_fused<float, 4, 8, 1, 2, 512, false, false>(prm, st);
     case (4 << 16) | (8 << 8) | 1: return launch_fused<float, 4, 8, 2, 4, 512, false, false>(prm, st);
+    case (4 << 16) | (8 << 8) | 2: return launch_fused<float, 4, 8, 1, 1, 256, false, false>(prm, st);
+    case (4 << 16) | (8 << 8) | 3: return launch_fused<float, 4, 8, 1, 4, 1024, false, false>(prm, st);
     case (5 << 16) | (8 << 8) | 0: return launch_fused<float, 5, 8, 2, 2, 512, false, false>(prm, st);
     case (5 << 16) | (8 << 8) | 1: return launch_fused<float, 5, 8, 1, 1, 512, false, false>(prm, st);
     case (5 << 16) | (8 << 8) | 2: return launch_fused<float, 5, 8, 2, 1, 256, false, false>(prm, st);
     case (5 << 16) | (8 << 8) | 3: return launch_fused<float, 5, 8, 4, 4, 512, false, false>(prm, st);
     case (5 << 16) | (8 << 8) | 4: return launch_fused<float, 5, 8, 2, 4, 1024, false, false>(prm, st);
-    case (6 << 16) | (7 << 8) | 0: return launch_fused<float, 6, 7, 1, 1, 512, false, false>(prm, st);
-    case (6 << 16) | (7 << 8) | 1: return launch_fused<float, 6, 7, 2, 2, 512, false, false>(prm, st);
+    case (5 << 16) | (8 << 8) | 5: return launch_fused<float, 5, 8, 1, 2, 1024, false, false>(prm, st);
+    case (6 << 16) | (7 << 8) | 0: return launch_fused<float, 6, 7, 2, 2, 512, false, false>(prm, st);
+    case (6 << 16) | (7 << 8) | 1: return launch_fused<float, 6, 7, 1, 1, 512, false, false>(prm, st);
+    case (6 << 16) | (7 << 8) | 2: return launch_fused<float, 6, 7, 1, 2, 1024, false, false>(prm, st);
     case (6 << 16) | (8 << 8) | 0: return launch_fused<float, 6, 8, 4, 2, 512, false, false>(prm, st);
     case (6 << 16) | (8 << 8) | 1: return launch_fused<float, 6, 8, 2, 1, 512, false, false>(prm, st);
     case (6 << 16) | (8 << 8) | 2: return launch_fused<float, 6, 8, 1, 1, 1024, false, false>(prm, st);
@@ -49,10 +55,10 @@ int fused_variants_c64(int logvec, int logm) {
     case (4 << 8) | 6: return 2;
     case (2 << 8) | 7: return 4;
     case (5 << 8) | 6: return 1;
-    case (5 << 8) | 7: return 3;
-    case (4 << 8) | 8: return 2;
-    case (5 << 8) | 8: return 5;
-    case (6 << 8) | 7: return 2;
+    case (5 << 8) | 7: return 5;
+    case (4 << 8) | 8: return 4;
+    case (5 << 8) | 8: return 6;
+    case (6 << 8) | 7: return 3;
     case (6 << 8) | 8: return 6;
     default: return 0;
     }
@@ -64,10 +70,13 @@ int fused_interleave_lg_c64(int logvec, int logm, int variant) {
     case (5 << 16) | (7 << 8) | 0: return 1;
     case (5 << 16) | (7 << 8) | 1: return 1;
     case (5 << 16) | (7 << 8) | 2: return 2;
+    case (5 << 16) | (7 << 8) | 4: return 2;
     case (5 << 16) | (8 << 8) | 0: return 1;
     case (5 << 16) | (8 << 8) | 3: return 2;
     case (5 << 16) | (8 << 8) | 4: return 2;
-    case (6 << 16) | (7 << 8) | 1: return 1;
+    case (5 << 16) | (8 << 8) | 5: return 1;
+    case (6 << 16) | (7 << 8) | 0: return 1;
+    case (6 << 16) | (7 << 8) | 2: return 1;
     case (6 << 16) | (8 << 8) | 0: return 1;
     case (6 << 16) | (8 << 8) | 3: return 2;
     case (6 << 16) | (8 << 8) | 4: return 2;
@@ -79,6 +88,8 @@ int fused_interleave_lg_c64(int logvec, int logm, int variant) {
 int fused_fwd_oop_c64(int logvec, int logm, int *vx, int *vy, int *lg) {
     switch ((logvec << 8) | logm) {
     case (6 << 8) | 8: *vx = 2; *vy = 2; *lg = 3; return 1;
+    case (5 << 8) | 8: *vx = 5; *vy = 5; *lg = 1; return 1;
+    case (6 << 8) | 7: *vx = 2; *vy = 2; *lg = 1; return 1;
     default: return 0;
     }
 }

@@ -21,15 +21,21 @@ cudaError_t launch_fused_c64_inv(const LineParams &prm, cudaStream_t st, bool *h
     case (5 << 16) | (7 << 8) | 0: return launch_fused<float, 5, 7, 1, 2, 512, true, false>(prm, st);
     case (5 << 16) | (7 << 8) | 1: return launch_fused<float, 5, 7, 2, 2, 256, true, false>(prm, st);
     case (5 << 16) | (7 << 8) | 2: return launch_fused<float, 5, 7, 2, 4, 512, true, false>(prm, st);
+    case (5 << 16) | (7 << 8) | 3: return launch_fused<float, 5, 7, 1, 1, 256, true, false>(prm, st);
+    case (5 << 16) | (7 << 8) | 4: return launch_fused<float, 5, 7, 1, 4, 1024, true, false>(prm, st);
     case (4 << 16) | (8 << 8) | 0: return launch_fused<float, 4, 8, 1, 2, 512, true, false>(prm, st);
     case (4 << 16) | (8 << 8) | 1: return launch_fused<float, 4, 8, 2, 4, 512, true, false>(prm, st);
+    case (4 << 16) | (8 << 8) | 2: return launch_fused<float, 4, 8, 1, 1, 256, true, false>(prm, st);
+    case (4 << 16) | (8 << 8) | 3: return launch_fused<float, 4, 8, 1, 4, 1024, true, false>(prm, st);
     case (5 << 16) | (8 << 8) | 0: return launch_fused<float, 5, 8, 2, 2, 512, true, false>(prm, st);
     case (5 << 16) | (8 << 8) | 1: return launch_fused<float, 5, 8, 1, 1, 512, true, false>(prm, st);
     case (5 << 16) | (8 << 8) | 2: return launch_fused<float, 5, 8, 2, 1, 256, true, false>(prm, st);
     case (5 << 16) | (8 << 8) | 3: return launch_fused<float, 5, 8, 4, 4, 512, true, false>(prm, st);
     case (5 << 16) | (8 << 8) | 4: return launch_fused<float, 5, 8, 2, 4, 1024, true, false>(prm, st);
-    case (6 << 16) | (7 << 8) | 0: return launch_fused<float, 6, 7, 1, 1, 512, true, false>(prm, st);
-    case (6 << 16) | (7 << 8) | 1: return launch_fused<float, 6, 7, 2, 2, 512, true, false>(prm, st);
+    case (5 << 16) | (8 << 8) | 5: return launch_fused<float, 5, 8, 1, 2, 1024, true, false>(prm, st);
+    case (6 << 16) | (7 << 8) | 0: return launch_fused<float, 6, 7, 2, 2, 512, true, false>(prm, st);
+    case (6 << 16) | (7 << 8) | 1: return launch_fused<float, 6, 7, 1, 1, 512, true, false>(prm, st);
+    case (6 << 16) | (7 << 8) | 2: return launch_fused<float, 6, 7, 1, 2, 1024, true, false>(prm, st);
     case (6 << 16) | (8 << 8) | 0: return launch_fused<float, 6, 8, 4, 2, 512, true, false>(prm, st);
     case (6 << 16) | (8 << 8) | 1: return launch_fused<float, 6, 8, 2, 1, 512, true, false>(prm, st);
     case (6 << 16) | (8 << 8) | 2: return launch_fused<float, 6, 8, 1, 1, 1024, true, false>(prm, st);
