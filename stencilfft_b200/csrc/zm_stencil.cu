@@ -68,10 +68,18 @@ template <typename S> struct vec16 {
 // OP = ST_ALL (2D): the Laplacian (coef) into `out`, dx and dy (coef2 = delta) into
 // `out2` / `out3` from one read of the neighbourhood; each result is computed exactly as
 // by its own kernel.
+// dx / dy divide by 12 delta.  FP64 divides, as the reference does (dx.cu:79), so the
+// results are bit-identical to it; FP32 (no reference counterpart) multiplies by
+// rden = 1 / (12 delta), computed in FP64 and rounded once, at most one ulp from the
+// quotient and a fraction of the cost of a correctly rounded FP32 division.
+template <typename S> ZM_DEV S div_den(S x, S den, S rden);
+template <> ZM_DEV double div_den<double>(double x, double den, double) { return __ddiv_rn(x, den); }
+template <> ZM_DEV float div_den<float>(float x, float, float rden) { return __fmul_rn(x, rden); }
+
 template <typename S, int NC, int OP, int DIM>
 __global__ void __launch_bounds__(256) stencil_kernel(const S *__restrict__ in, S *__restrict__ out,
                                                       S *__restrict__ out2, S *__restrict__ out3,
-                                                      const Geom g, int64_t nvec, S coef, S coef2) {
+                                                      const Geom g, int64_t nvec, S coef, S coef2, S rden) {
     using O = ops<S>;
     using V = vec16<S>;
     constexpr int K = V::n / NC;                 // elements per vector
@@ -173,12 +181,12 @@ __global__ void __launch_bounds__(256) stencil_kernel(const S *__restrict__ in, 
             x = O::add(x, lf2.v[i]);
             x = O::add(x, O::mul(rt.v[i], (S)8));
             x = O::sub(x, rt2.v[i]);
-            rx.v[i] = O::div(x, den);
+            rx.v[i] = div_den(x, den, rden);
             S y = O::add((S)0, O::mul(up.v[i], (S)-8));
             y = O::add(y, up2.v[i]);
             y = O::add(y, O::mul(dn.v[i], (S)8));
             y = O::sub(y, dn2.v[i]);
-            ry.v[i] = O::div(y, den);
+            ry.v[i] = div_den(y, den, rden);
         }
         *reinterpret_cast<uint4 *>(out2 + e * NC) = *reinterpret_cast<const uint4 *>(&rx);
         *reinterpret_cast<uint4 *>(out3 + e * NC) = *reinterpret_cast<const uint4 *>(&ry);
@@ -219,7 +227,7 @@ __global__ void __launch_bounds__(256) stencil_kernel(const S *__restrict__ in, 
             s = O::add(s, m2.v[i]);
             s = O::add(s, O::mul(p1.v[i], (S)8));
             s = O::sub(s, p2.v[i]);
-            res.v[i] = O::div(s, den);
+            res.v[i] = div_den(s, den, rden);
         }
     }
     *reinterpret_cast<uint4 *>(out + e * NC) = *reinterpret_cast<const uint4 *>(&res);
@@ -236,18 +244,21 @@ static cudaError_t launch_s(const zm_plan_s *p, int op, const void *in, void *ou
     const S *i = reinterpret_cast<const S *>(in);
     S *o = reinterpret_cast<S *>(out), *o2 = reinterpret_cast<S *>(out2), *o3 = reinterpret_cast<S *>(out3);
     const S c = (S)coef, c2 = (S)coef2;
+    // 1 / (12 delta) for the FP32 derivatives (delta = coef for dx / dy, coef2 for ST_ALL)
+    const double dl = op == ST_ALL ? coef2 : coef;
+    const S rd = (S)(1.0 / (12.0 * dl));
     if (p->g.dim == 2) {
         if (op == ST_LAPLACE)
-            stencil_kernel<S, NC, ST_LAPLACE, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2);
+            stencil_kernel<S, NC, ST_LAPLACE, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
         else if (op == ST_DX)
-            stencil_kernel<S, NC, ST_DX, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2);
+            stencil_kernel<S, NC, ST_DX, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
         else if (op == ST_DY)
-            stencil_kernel<S, NC, ST_DY, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2);
+            stencil_kernel<S, NC, ST_DY, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
         else
-            stencil_kernel<S, NC, ST_ALL, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2);
+            stencil_kernel<S, NC, ST_ALL, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
     } else {
         if (op != ST_LAPLACE) return cudaErrorInvalidValue;
-        stencil_kernel<S, NC, ST_LAPLACE, 3><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2);
+        stencil_kernel<S, NC, ST_LAPLACE, 3><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
     }
     count_launch();
     return cudaGetLastError();
