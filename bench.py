@@ -429,6 +429,15 @@ def run_profile_case(args):
     modes, amps = modes_and_amps(n)
     u = pl.empty()
     pl.fill_modes(u, modes, amps, NOISE, NOISE_SEED)
+    if args.profile_ops == "inv":
+        # inverse transform only (with a workspace): three buffers on the device
+        back, work = pl.empty(), pl.empty()
+        for _ in range(2):
+            pl.inverse_fft(u, back, scale=1.0 / (n * n), work=work)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": {"n": n, "p": P, "b": B, "dtype": args.profile_dtype,
+                                           "ops": "inv", "field_bytes": pl.field_bytes}}))
+        return
     if args.profile_ops == "fwd":
         # forward transform only (with a workspace, as in the timed step): three buffers
         spec, work = pl.empty(), pl.empty()
@@ -460,7 +469,7 @@ def main():
                     help="run the small profiling case only (for ncu captures)")
     ap.add_argument("--profile-n", type=int, default=8192)
     ap.add_argument("--profile-dtype", default="c64")
-    ap.add_argument("--profile-ops", choices=["all", "fwd"], default="all")
+    ap.add_argument("--profile-ops", choices=["all", "fwd", "inv"], default="all")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.profile_case:
