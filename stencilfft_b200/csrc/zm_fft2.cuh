@@ -17,8 +17,10 @@
 //     butterfly sits at a compile-time offset from its base;
 //   * each sub-transform is at most two register stages of radix <= 16 (Stockham
 //     indexing), with the stage twiddles w_VEC, w_M in shared memory and the inter-step
-//     twiddle w_N^{n1 k2} from two shared-memory factor tables (complex64 with one CTA
-//     per tile: two compensated products) or an FP64 power walk;
+//     twiddle w_N^{n1 k2} as two compensated products in complex64 tiles held by one
+//     CTA -- forward with two 16-point column stages: w_N^{j k2} w_N^{16 r k2} read
+//     through L1 by lanes that share k2; otherwise two shared-memory factor tables --
+//     or an FP64 power walk;
 //   * one tile per cluster, the vector side moved through registers / 16-byte vectors;
 //     or, for forward passes with two row stages in the persistent variants (PERS), a
 //     cluster walks tiles c, c + clusters, ... and each CTA fetches the vector-side rows
@@ -26,7 +28,9 @@
 //     mbarrier with a bounded wait) into a staging buffer as soon as the current tile's
 //     first row stage has read it, so HBM reads overlap the rest of the tile;
 //   * the frequency side is read / written straight from registers with lanes ordered
-//     so that a warp covers whole sectors.
+//     so that a warp covers whole sectors;
+//   * a forward tile asks for an L2 prefetch (cp.async.bulk.prefetch) of the vector
+//     side of the tile one wave of clusters ahead.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -87,6 +91,13 @@ ZM_DEV void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) 
                  : "memory");
 }
 constexpr unsigned long long kCopyWaitNs = 1000000000ull;   // 1 s
+// hint: bring [src, src + bytes) into L2 (no completion to wait for); 16-byte aligned,
+// bytes a multiple of 16
+ZM_DEV void bulk_prefetch_l2(const void *src, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"((unsigned long long)__cvta_generic_to_global(src)),
+                 "r"(bytes)
+                 : "memory");
+}
 
 // Shared-memory geometry and radix split of one CTA's slice.
 template <int LV, int LM, int CL, int TL, int NT> struct SliceGeom {
@@ -119,6 +130,11 @@ template <int LV, int LM, int CL, int TL, int NT> struct SliceGeom {
     static constexpr int LOGN = LV + LM, TLO = LOGN / 2;
     static constexpr int NTA = 1 << (LOGN - TLO), NTB = 1 << TLO;
     template <typename T> static constexpr bool twtab() { return sizeof(T) == 4 && CL == 1; }
+    // complex64 one-CTA forward tiles with two 16-point column stages: the first column
+    // stage runs with lanes along n1 mod 16 and splits w_N^{(j + 16 r) k2} into
+    // w_N^{j k2} (once per unit) and w_N^{16 r k2} (the same for the 16 lanes of one k2),
+    // both read through L1 from the plan's hi/lo table (no per-CTA table fill)
+    template <typename T> static constexpr bool colq() { return twtab<T>() && RC2 == 16 && VEC > 4; }
     static constexpr int smax(int a, int b) { return a > b ? a : b; }
     static constexpr int STAGE_ELEMS = smax(stage_elems(1), smax(stage_elems(2), stage_elems(4)));
 };
@@ -204,7 +220,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
         const Wt *tv = reinterpret_cast<const Wt *>(prm.twv);
         const Wt *tm = reinterpret_cast<const Wt *>(prm.twm);
         for (int i = tid; i < VEC + M; i += NT) stv[i] = i < VEC ? ldtw(tv, i) : ldtw(tm, i - VEC);
-        if constexpr (SG::template twtab<T>()) {
+        if constexpr (SG::template twtab<T>() && (INV || !SG::template colq<T>())) {
             const double2 *td = reinterpret_cast<const double2 *>(prm.twd);
             for (int i = tid; i < SG::NTA + SG::NTB; i += NT)
                 sta[i] = tw_from_d<T>(ldd2(td + (i < SG::NTA ? (i << SG::TLO) : i - SG::NTA)));
@@ -374,6 +390,55 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
 
     // ---- forward: w_N^{n1 k2}, M-point column transforms over n1, frequency-side store
     auto fwd_columns = [&]() {
+      if constexpr (SG::template colq<T>()) {
+        // complex64, one CTA per tile, RC2 = 16: the first stage runs with lanes along
+        // j = n1 mod RC2 (k2 = zk with CL = 1); unit (t, k2, j) transforms n1 = j + RC2 r,
+        // twiddled by w_N^{j k2} (one lookup per unit) times w_N^{RC2 r k2} (a lookup
+        // shared by the lanes of one k2); its outputs s go to column position s RC2 + j,
+        // so the second stage reads each unit's RC2 points as one run
+        const Wt *twn = reinterpret_cast<const Wt *>(prm.twN);   // hi/lo pairs of w_N^m
+        constexpr int NU = EPT / RC1;
+        C z[NU][RC1];
+        int zt[NU], zk[NU], zj[NU];
+#pragma unroll
+        for (int i = 0; i < NU; i++) {
+            const int u = tid + i * NT;
+            zj[i] = u % RC2;
+            const int rr = u / RC2;
+            zk[i] = rr % VL;
+            zt[i] = rr / VL;
+            const Wt b = ldtw(twn, zj[i] * zk[i]);
+#pragma unroll
+            for (int r = 0; r < RC1; r++) {
+                const C x = twmul<false>(S[SG::Y(zt[i], zk[i], zj[i] + RC2 * r)], b);
+                z[i][r] = r == 0 ? x : twmul<false>(x, ldtw(twn, RC2 * r * zk[i]));
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < NU; i++) dft<RC1, DIR, T>(z[i]);
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < NU; i++)
+#pragma unroll
+            for (int r = 0; r < RC1; r++) S[SG::Y(zt[i], zk[i], r * RC2 + zj[i])] = z[i][r];
+        __syncthreads();
+        constexpr int NU2 = EPT / RC2;
+#pragma unroll
+        for (int i = 0; i < NU2; i++) {
+            const int u = tid + i * NT;
+            int t, k2l, j2;
+            colunit(u, RC1, t, k2l, j2);
+            C y[RC2];
+#pragma unroll
+            for (int r = 0; r < RC2; r++) y[r] = S[SG::Y(t, k2l, j2 * RC2 + r)];
+#pragma unroll
+            for (int r = 1; r < RC2; r++) y[r] = twmul<false>(y[r], stm[j2 * r]);
+            dft<RC2, DIR, T>(y);
+            C *op = fptr(out, t, k2l, j2);
+#pragma unroll
+            for (int r = 0; r < RC2; r++) op[fstep2 * r] = scale_c(y[r]);
+        }
+      } else {
         constexpr int NU = EPT / RC1;
         C z[NU][RC1];
         int zt[NU], zk[NU], zj[NU];
@@ -426,6 +491,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
                 for (int r = 0; r < RC2; r++) op[fstep2 * r] = scale_c(y[r]);
             }
         }
+      }
     };
 
     if constexpr (fused_persistent<T, LV, LM, CL, TL, NT, INV, PERS>()) {
@@ -496,6 +562,26 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
         return;
     } else {
         set_tile((int64_t)(blockIdx.x / CL) * TL);
+        // forward: L2 prefetch of the vector side of the tile one wave of clusters ahead,
+        // so its HBM reads overlap this tile's work (for an interleaved intermediate the
+        // first line of each group fetches the group's runs).  Measured on the inverse
+        // passes' frequency side it did not pay, so they take none.
+        const int64_t ft = (int64_t)(blockIdx.x / CL) + prm.pf_tiles;
+        if (!INV && prm.pf_tiles > 0 && rank == 0 && ft < prm.nlines / TL) {
+            const int nch = (int)(SG::N >> logL);                  // rank chunks per line
+            if (tid < TL * nch) {
+                const int t = tid / nch, c = tid - t * nch;
+                const int64_t l = ft * TL + t;
+                if (a0.a_pos == 1 || (l & (a0.a_pos - 1)) == 0) {
+                    const LineAddr a = line_addr(g, prm.kind, l, prm.lg_inter);
+                    const unsigned char *src = reinterpret_cast<const unsigned char *>(in + a.a_base + c * a.a_chunk);
+                    const int64_t bytes = L * a0.a_pos * (int64_t)sizeof(C);
+                    if (((uintptr_t)src & 15) == 0 && (bytes & 15) == 0)
+                        for (int64_t o = 0; o < bytes; o += 32768)
+                            bulk_prefetch_l2(src + o, (unsigned)(bytes - o < 32768 ? bytes - o : 32768));
+                }
+            }
+        }
         __syncthreads();
     }
 
@@ -733,17 +819,17 @@ cudaError_t launch_fused(const LineParams &prm, cudaStream_t st) {
     if (!attr_done[dev]) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        if (persistent) {
-            clusters[dev] = resident_clusters<CL, NT>(kern, smem, dev);
-            if (clusters[dev] <= 0) return cudaErrorInvalidConfiguration;
-        }
+        clusters[dev] = resident_clusters<CL, NT>(kern, smem, dev);
+        if (clusters[dev] <= 0) return cudaErrorInvalidConfiguration;
         attr_done[dev] = 1;
     }
     const int64_t ntiles = prm.nlines / TL;
     const int64_t nclus = persistent ? (ntiles < clusters[dev] ? ntiles : clusters[dev]) : ntiles;
     const unsigned grid = (unsigned)nclus * CL;
+    LineParams lp = prm;
+    lp.pf_tiles = persistent ? 0 : clusters[dev];   // one wave of resident clusters ahead
     if constexpr (CL == 1) {
-        kern<<<grid, NT, smem, st>>>(prm);
+        kern<<<grid, NT, smem, st>>>(lp);
     } else {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(grid);
@@ -757,7 +843,7 @@ cudaError_t launch_fused(const LineParams &prm, cudaStream_t st) {
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        cudaError_t e = cudaLaunchKernelEx(&cfg, kern, prm);
+        cudaError_t e = cudaLaunchKernelEx(&cfg, kern, lp);
         if (e != cudaSuccess) return e;
     }
     count_launch();

@@ -41,6 +41,7 @@ struct LineParams {
     int permute_only;  // skip all arithmetic (reference do_compute=false)
     int lg_inter;      // 2D: log2 of the row interleave of the x -> y intermediate (0 = plain REPACK layout)
     int *err;          // device word set to 1 when a bounded wait inside a kernel gives up
+    int64_t pf_tiles;  // size-specialised passes: L2 prefetch distance in tiles (0 = none)
     // radix schedules of the two sub-transforms (first stage first)
     int nst_vec, nst_m;
     int rad_vec[8], rad_m[8];
