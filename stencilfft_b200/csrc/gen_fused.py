@@ -1,7 +1,9 @@
 """Generates zm_fft2_<dtype>_<dir>.cu: the size-specialised fused passes and their
 dispatch tables.  Each (log2 VEC, log2 M) pair lists variants (cluster size CL, lines
 per tile TL, threads NT[, "p" = persistent forward pass with bulk-copy prefetch]); the
-plan's `variant` picks one.  Variant 0, the default, is
+plan's `variant` picks one; "k3" marks the three-stage 512-thread pass of zm_fft3.cuh
+for complex64 lines of 2^14 points ("k3p": its persistent form with asynchronous copies
+of the next line).  Variant 0, the default, is
 the fastest one measured on B200 at the sizes the table was tuned on; zm_plan_autotune
 re-measures them for a plan."""
 VARIANTS = {
@@ -12,7 +14,8 @@ VARIANTS = {
         (4, 8): [(1, 2, 512), (2, 4, 512), (1, 1, 256), (1, 4, 1024)],
         (5, 8): [(2, 2, 512), (1, 1, 512), (2, 1, 256), (4, 4, 512), (2, 4, 1024), (1, 2, 1024)],
         (6, 7): [(2, 2, 512), (1, 1, 512), (1, 2, 1024)],
-        (6, 8): [(4, 2, 512), (2, 1, 512), (1, 1, 1024), (8, 4, 512), (4, 4, 1024), (4, 2, 512, "p")],
+        (6, 8): [(4, 2, 512), (2, 1, 512), (1, 1, 1024), (8, 4, 512), (4, 4, 1024), (4, 2, 512, "p"),
+                 (1, 1, 512, "k3"), (1, 1, 512, "k3p")],
     },
     "c128": {
         (4, 4): [(1, 16, 256)], (4, 5): [(1, 8, 256)], (4, 6): [(1, 4, 256)], (2, 7): [(1, 8, 256), (1, 4, 128), (1, 16, 512)],
@@ -27,7 +30,16 @@ VARIANTS = {
 # one 1024-thread CTA per line in both passes with 8-row interleave, 3.73 ms per forward
 # transform against 4.61 for the in-place default.
 FWD_OOP = {
-    "c64": {(6, 8): (2, 2, 3), (5, 8): (5, 5, 1), (6, 7): (2, 2, 1)},
+    "c64": {(6, 8): (7, 2, 3), (5, 8): (5, 5, 1), (6, 7): (2, 2, 1)},
+    "c128": {},
+}
+# Out-of-place 2D inverse configurations (caller workspace, default variant): y pass
+# variant (frequency side -> work), x pass variant (work -> vector side), log2 of the
+# row interleave.  Measured on B200 at N = 16384, P = 4, B = 64 (c64): y pass on 2-line
+# tiles of a 4-CTA cluster, x pass on the persistent three-stage kernel, 8-row
+# interleave: 3.24 ms against 3.40 for the in-place default.
+INV_OOP = {
+    "c64": {(6, 8): (0, 7, 3)},
     "c128": {},
 }
 T = {"c64": "float", "c128": "double"}
@@ -36,7 +48,8 @@ for dt, table in VARIANTS.items():
         d = "inv" if inv else "fwd"
         L = [f"// zm_fft2_{dt}_{d}.cu -- generated by gen_fused.py: size-specialised fused axis passes,",
              f"// {dt}, {'inverse' if inv else 'forward'} direction (kernel template in zm_fft2.cuh).",
-             '#include "zm_internal.h"', '#include "zm_lines.cuh"', '#include "zm_fft2.cuh"', "",
+             '#include "zm_internal.h"', '#include "zm_lines.cuh"', '#include "zm_fft2.cuh"',
+             '#include "zm_fft3.cuh"', "",
              "namespace zm {", "",
              f"cudaError_t launch_fused_{dt}_{d}(const LineParams &prm, cudaStream_t st, bool *handled) {{",
              "    *handled = true;",
@@ -45,6 +58,11 @@ for dt, table in VARIANTS.items():
             for vi, v in enumerate(vs):
                 cl, tl, nt = v[:3]
                 pers = "true" if len(v) > 3 and v[3] == "p" else "false"
+                if len(v) > 3 and v[3] in ("k3", "k3p"):
+                    L.append(f"    case ({lv} << 16) | ({lm} << 8) | {vi}: "
+                             f"return launch_k3<{lv}, {lm}, {'true' if inv else 'false'}, "
+                             f"{'true' if v[3] == 'k3p' else 'false'}>(prm, st);")
+                    continue
                 L.append(f"    case ({lv} << 16) | ({lm} << 8) | {vi}: "
                          f"return launch_fused<{T[dt]}, {lv}, {lm}, {cl}, {tl}, {nt}, {'true' if inv else 'false'}, {pers}>(prm, st);")
         L += ["    default: break;", "    }", "    *handled = false;", "    return cudaSuccess;", "}", ""]
@@ -72,10 +90,12 @@ for dt, table in VARIANTS.items():
                     if g >= 2 and ra2 > 1:
                         L.append(f"    case ({lv} << 16) | ({lm} << 8) | {vi}: return {g.bit_length() - 1};")
             L += ["    default: return 0;", "    }", "}", ""]
-            L += [f"int fused_fwd_oop_{dt}(int logvec, int logm, int *vx, int *vy, int *lg) {{",
-                  "    switch ((logvec << 8) | logm) {"]
-            for (lv, lm), (vx, vy, lg) in FWD_OOP[dt].items():
-                L.append(f"    case ({lv} << 8) | {lm}: *vx = {vx}; *vy = {vy}; *lg = {lg}; return 1;")
-            L += ["    default: return 0;", "    }", "}", ""]
+            for name, oop in (("fwd", FWD_OOP), ("inv", INV_OOP)):
+                L += [f"int fused_{name}_oop_{dt}(int logvec, int logm, int *vx, int *vy, int *lg) {{",
+                      "    switch ((logvec << 8) | logm) {"]
+                for (lv, lm), (v1, v2, lg) in oop[dt].items():
+                    a, b = (v1, v2) if name == "fwd" else (v2, v1)
+                    L.append(f"    case ({lv} << 8) | {lm}: *vx = {a}; *vy = {b}; *lg = {lg}; return 1;")
+                L += ["    default: return 0;", "    }", "}", ""]
         L += ["}  // namespace zm", ""]
         open(f"zm_fft2_{dt}_{d}.cu", "w").write("\n".join(L))

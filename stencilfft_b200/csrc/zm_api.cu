@@ -188,6 +188,16 @@ static bool fwd_oop_config(const zm_plan_s *p, int *vx, int *vy, int *lg) {
     if (*lg > p->g.logVP) *lg = p->g.logVP;
     return true;
 }
+// The out-of-place inverse configuration of a 2D plan (y pass in -> work, x pass
+// work -> out), or false.
+static bool inv_oop_config(const zm_plan_s *p, int *vx, int *vy, int *lg) {
+    if (p->g.dim != 2 || (p->flags & ZM_FLAG_PERMUTE_ONLY) || p->nvariants == 0 || p->variant != 0) return false;
+    const int ok = p->dtype == ZM_C128 ? zm::fused_inv_oop_c128(p->g.logVEC, p->g.logM, vx, vy, lg)
+                                       : zm::fused_inv_oop_c64(p->g.logVEC, p->g.logM, vx, vy, lg);
+    if (!ok) return false;
+    if (*lg > p->g.logVP) *lg = p->g.logVP;
+    return true;
+}
 
 // `variant` / `lg` >= 0 override the plan's tile shape and row interleave for this pass.
 static int run_pass(const zm_plan_s *p, int kind, bool inv, const void *in, void *out, bool scale,
@@ -253,6 +263,11 @@ static int inverse_impl(zm_plan p, const void *in, void *out, void *work, double
         return fail(ZM_ERR_INVALID_ARG, "work overlaps in/out");
     void *tmp = work ? work : const_cast<void *>(in);
     if (p->g.dim == 2) {
+        int vx, vy, lg;
+        if (work && inv_oop_config(p, &vx, &vy, &lg)) {
+            if ((rc = run_pass(p, zm::PASS_Y2, true, in, work, false, 0, 0, st, vy, lg))) return rc;
+            return run_pass(p, zm::PASS_X2, true, work, out, true, sre, sim, st, vx, lg);
+        }
         if ((rc = run_pass(p, zm::PASS_Y2, true, in, tmp, false, 0, 0, st))) return rc;
         return run_pass(p, zm::PASS_X2, true, tmp, out, true, sre, sim, st);
     }

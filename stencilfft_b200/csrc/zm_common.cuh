@@ -91,32 +91,37 @@ template <> ZM_DEV cpx<float> ldg(const cpx<float> *p) {
 
 // ----------------------------------------------------- radix-R DFT codelets
 // Constant twiddles w_R^k = exp(DIR * 2 pi i k / R), DIR = -1 forward, +1 inverse.
-// cos(2 pi k / 16) for k = 0..4 (cos pi/8, cos pi/4, cos 3pi/8).
-struct k16 {
-    static constexpr double c1 = 0.92387953251128675613;  // cos(pi/8)
-    static constexpr double c2 = 0.70710678118654752440;  // cos(pi/4)
-    static constexpr double c3 = 0.38268343236508977173;  // cos(3pi/8)
+// cos(2 pi j / 32) for j = 0..8, the first octant of the 32-point circle.
+struct k32 {
+    static constexpr double c[9] = {1.0,
+                                    0.98078528040323044913,    // cos(pi/16)
+                                    0.92387953251128675613,    // cos(pi/8)
+                                    0.83146961230254523708,    // cos(3pi/16)
+                                    0.70710678118654752440,    // cos(pi/4)
+                                    0.55557023301960222474,    // cos(5pi/16)
+                                    0.38268343236508977173,    // cos(3pi/8)
+                                    0.19509032201612826785,    // cos(7pi/16)
+                                    0.0};
 };
 
 template <int R, int K, int DIR, typename T> ZM_DEV cpx<T> cmul_const(cpx<T> v) {
     constexpr int k = ((K % R) + R) % R;
-    constexpr int k16i = k * (16 / R);        // position on the 16-point circle (R <= 16)
-    static_assert(16 % R == 0, "radix must divide 16");
-    if constexpr (k16i == 0) {
+    constexpr int kc = k * (32 / R);          // position on the 32-point circle (R <= 32)
+    static_assert(32 % R == 0, "radix must divide 32");
+    if constexpr (kc == 0) {
         return v;
-    } else if constexpr (k16i == 8) {
+    } else if constexpr (kc == 16) {
         return {-v.x, -v.y};
-    } else if constexpr (k16i == 4) {          // DIR=-1: -i, DIR=+1: +i
+    } else if constexpr (kc == 8) {            // DIR=-1: -i, DIR=+1: +i
         return DIR < 0 ? cpx<T>{v.y, -v.x} : cpx<T>{-v.y, v.x};
-    } else if constexpr (k16i == 12) {
+    } else if constexpr (kc == 24) {
         return DIR < 0 ? cpx<T>{-v.y, v.x} : cpx<T>{v.y, -v.x};
     } else {
         // general: (c + DIR*i*s)
-        constexpr double cs[5] = {1.0, k16::c1, k16::c2, k16::c3, 0.0};
-        constexpr int q = k16i % 8;            // angle in (0, pi) modulo pi
-        constexpr double c0 = q <= 4 ? cs[q] : -cs[8 - q];
-        constexpr double s0 = q <= 4 ? cs[4 - q] : cs[q - 4];
-        constexpr double sgn = k16i >= 8 ? -1.0 : 1.0;   // add pi
+        constexpr int q = kc % 16;             // angle in (0, pi) modulo pi
+        constexpr double c0 = q <= 8 ? k32::c[q] : -k32::c[16 - q];
+        constexpr double s0 = q <= 8 ? k32::c[8 - q] : k32::c[q - 8];
+        constexpr double sgn = kc >= 16 ? -1.0 : 1.0;    // add pi
         constexpr double cc = sgn * c0, ss = sgn * s0 * (DIR < 0 ? -1.0 : 1.0);
         const T c = (T)cc, s = (T)ss;
         return {v.x * c - v.y * s, v.x * s + v.y * c};

@@ -811,6 +811,11 @@ cudaError_t launch_fused(const LineParams &prm, cudaStream_t st) {
     constexpr size_t smem = fused_smem_bytes<T, LV, LM, CL, TL, NT, INV, PERS>();
     static_assert(smem <= 227 * 1024, "shared memory of one CTA");
     constexpr bool persistent = fused_persistent<T, LV, LM, CL, TL, NT, INV, PERS>();
+    // the staging rows of a persistent pass hold sg = 1, 2 or 4 interleaved lines and
+    // are sized for sg <= TL: a wider interleave of the y pass's vector side is refused
+    if (persistent && prm.kind == PASS_Y2 && prm.lg_inter > 0 &&
+        ((1 << prm.lg_inter) > TL || prm.lg_inter > 2))
+        return cudaErrorInvalidValue;
     auto kern = fused_pass_kernel<T, LV, LM, CL, TL, NT, INV, PERS>;
     static int attr_done[64], clusters[64];
     int dev = 0;

@@ -3,6 +3,7 @@
 #include "zm_internal.h"
 #include "zm_lines.cuh"
 #include "zm_fft2.cuh"
+#include "zm_fft3.cuh"
 
 namespace zm {
 
@@ -59,6 +60,12 @@ int fused_interleave_lg_c128(int logvec, int logm, int variant) {
 }
 
 int fused_fwd_oop_c128(int logvec, int logm, int *vx, int *vy, int *lg) {
+    switch ((logvec << 8) | logm) {
+    default: return 0;
+    }
+}
+
+int fused_inv_oop_c128(int logvec, int logm, int *vx, int *vy, int *lg) {
     switch ((logvec << 8) | logm) {
     default: return 0;
     }

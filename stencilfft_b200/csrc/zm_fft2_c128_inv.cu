@@ -3,6 +3,7 @@
 #include "zm_internal.h"
 #include "zm_lines.cuh"
 #include "zm_fft2.cuh"
+#include "zm_fft3.cuh"
 
 namespace zm {
 

@@ -3,6 +3,7 @@
 #include "zm_internal.h"
 #include "zm_lines.cuh"
 #include "zm_fft2.cuh"
+#include "zm_fft3.cuh"
 
 namespace zm {
 
@@ -42,6 +43,8 @@ cudaError_t launch_fused_c64_fwd(const LineParams &prm, cudaStream_t st, bool *h
     case (6 << 16) | (8 << 8) | 3: return launch_fused<float, 6, 8, 8, 4, 512, false, false>(prm, st);
     case (6 << 16) | (8 << 8) | 4: return launch_fused<float, 6, 8, 4, 4, 1024, false, false>(prm, st);
     case (6 << 16) | (8 << 8) | 5: return launch_fused<float, 6, 8, 4, 2, 512, false, true>(prm, st);
+    case (6 << 16) | (8 << 8) | 6: return launch_k3<6, 8, false, false>(prm, st);
+    case (6 << 16) | (8 << 8) | 7: return launch_k3<6, 8, false, true>(prm, st);
     default: break;
     }
     *handled = false;
@@ -59,7 +62,7 @@ int fused_variants_c64(int logvec, int logm) {
     case (4 << 8) | 8: return 4;
     case (5 << 8) | 8: return 6;
     case (6 << 8) | 7: return 3;
-    case (6 << 8) | 8: return 6;
+    case (6 << 8) | 8: return 8;
     default: return 0;
     }
 }
@@ -87,9 +90,16 @@ int fused_interleave_lg_c64(int logvec, int logm, int variant) {
 
 int fused_fwd_oop_c64(int logvec, int logm, int *vx, int *vy, int *lg) {
     switch ((logvec << 8) | logm) {
-    case (6 << 8) | 8: *vx = 2; *vy = 2; *lg = 3; return 1;
+    case (6 << 8) | 8: *vx = 7; *vy = 2; *lg = 3; return 1;
     case (5 << 8) | 8: *vx = 5; *vy = 5; *lg = 1; return 1;
     case (6 << 8) | 7: *vx = 2; *vy = 2; *lg = 1; return 1;
+    default: return 0;
+    }
+}
+
+int fused_inv_oop_c64(int logvec, int logm, int *vx, int *vy, int *lg) {
+    switch ((logvec << 8) | logm) {
+    case (6 << 8) | 8: *vx = 7; *vy = 0; *lg = 3; return 1;
     default: return 0;
     }
 }

@@ -36,6 +36,9 @@ int fused_interleave_lg_c128(int logvec, int logm, int variant);
 // configuration of (VEC, M), when there is one.
 int fused_fwd_oop_c64(int logvec, int logm, int *vx, int *vy, int *lg);
 int fused_fwd_oop_c128(int logvec, int logm, int *vx, int *vy, int *lg);
+// the same for the out-of-place 2D inverse (y pass in -> work, x pass work -> out)
+int fused_inv_oop_c64(int logvec, int logm, int *vx, int *vy, int *lg);
+int fused_inv_oop_c128(int logvec, int logm, int *vx, int *vy, int *lg);
 
 // zm_stencil.cu
 enum StencilOp : int { ST_LAPLACE = 0, ST_DX = 1, ST_DY = 2, ST_ALL = 3 };
