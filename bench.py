@@ -369,10 +369,11 @@ def run_ours(args, rank: int, world: int):
     e2e_ms = gmax(main["e2e_ms"])
     F = main["field_bytes"]
     peak, peak_kind = read_peaks()
-    # dominant kernel: the forward fused line pass (2 launches per forward call)
+    # dominant kernel: the three-stage fused line pass of the forward transform (2 launches
+    # per forward call: x pass persistent, y pass one line per CTA)
     t_launch = main["stage_ms"]["fwd"] / 2
     achieved = (2 * F) / (t_launch * 1e-3) / 1e9
-    traffic = read_traffic("fused_pass_fwd_c64_N16384")
+    traffic = read_traffic("k3_pass_fwd_c64_N16384")
     fft_flops = 5.0 * N * N * math.log2(N * N)
     # algorithmic bytes: 4F per 2D transform, 2F per stencil (6F for the three fused
     # stencils, which move 4F: one read, three writes)
@@ -394,7 +395,7 @@ def run_ours(args, rank: int, world: int):
         "config": {"workload": WORKLOAD, "n": N, "p": P, "b": B, "dtype": "c64 (compensated FP32 twiddles)",
                    "l2": "inputs larger than L2 (2 GiB field per buffer)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
-        "roofline": {"bound": "hbm", "kernel": "fused_pass_kernel<float,6,8,1,1,1024,fwd> (x and y axis passes)",
+        "roofline": {"bound": "hbm", "kernel": "k3_pass_kernel<6,8,fwd> (x pass persistent, y pass one line per CTA)",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "traffic": traffic, "algorithmic_bytes_per_launch": 2 * F},

@@ -90,7 +90,7 @@ int fused_interleave_lg_c64(int logvec, int logm, int variant) {
 
 int fused_fwd_oop_c64(int logvec, int logm, int *vx, int *vy, int *lg) {
     switch ((logvec << 8) | logm) {
-    case (6 << 8) | 8: *vx = 7; *vy = 2; *lg = 3; return 1;
+    case (6 << 8) | 8: *vx = 7; *vy = 6; *lg = 3; return 1;
     case (5 << 8) | 8: *vx = 5; *vy = 5; *lg = 1; return 1;
     case (6 << 8) | 7: *vx = 2; *vy = 2; *lg = 1; return 1;
     default: return 0;

@@ -86,8 +86,7 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
     constexpr int M = 1 << LM, VEC = 1 << LV;
     constexpr int HP = 512 / M;                 // threads per vector-side row n1 (stage 1 / C)
     constexpr int DSTEP = 1024 / M;             // n2 step between consecutive d2
-    constexpr int SROW = VEC + 4;               // staging row of the vector side (PERS)
-    static_assert(!PERS || M * SROW <= KG::EX, "staging rows fit the exchange region");
+    static_assert(!PERS || M * (VEC + 4) <= KG::EX, "staging rows fit the exchange region");
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *S = reinterpret_cast<C *>(smem_raw);
@@ -103,10 +102,21 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
     const int64_t lstep = PERS ? (int64_t)gridDim.x : nl;
     const int kind = prm.kind, lgi = prm.lg_inter;
 
-    // stage-1 / stage-C thread: vector-side row n1, units n2_lo = 2 h + b (b = 0, 1)
+    // stage-1 / stage-C thread: vector-side row n1 and two units n2_lo = lo0, lo1 (the
+    // line's positions n2 = n2_lo + DSTEP d2).  Contiguous vector side: lo1 = lo0 + 1, the
+    // two points of one d2 are one 16-byte vector.  Strided vector side (an interleaved
+    // intermediate): lanes h = 0, 1 take adjacent positions, so the 32 lanes of a load
+    // touch 16 cache lines instead of 32.
     const int h = tid % HP, n1 = tid / HP;
+    const LineAddr a0 = line_addr(g, kind, 0, lgi);
+    const int64_t apos = a0.a_pos;
+    const bool vcont = apos == 1;
+    const int lo0 = vcont ? 2 * h : h, lo1 = vcont ? 2 * h + 1 : h + HP;
     const int d0v = n1 & 31;
-    const int d1v = (n1 >> 5) + (M / 32) * (2 * h);    // d1 of unit b = 0 (b = 1: + M / 32)
+    const int d1v0 = (n1 >> 5) + (M / 32) * lo0, d1v1 = (n1 >> 5) + (M / 32) * lo1;
+    // staging row of the vector side (PERS): VEC + 4 elements keep the 16-byte reads of
+    // 16 rows per warp conflict-free, VEC + 2 the 8-byte reads of the strided form
+    const int srow = vcont ? VEC + 4 : VEC + 2;
     // stage-2 / stage-B thread: d0 = lane, ka = warp
     const int ka2 = warp;
     // stage-3 / stage-A thread: ka = tid & 15, kb = tid >> 4; k mod 512 = tid
@@ -120,9 +130,7 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
     // frequency side: element k = tid + 512 kc of line a is at fofs(a) + kc * fstep
     const int k2 = tid & (VEC - 1);
     const int64_t VP = g.vp;
-    const LineAddr a0 = line_addr(g, kind, 0, lgi);
     const int flg = a0.f_lg;
-    const int64_t apos = a0.a_pos;
     const int64_t pos0 = (int64_t)(tid >> LV) * VP + (k2 & (VP - 1));
     auto fofs = [&](const LineAddr &a) {
         return a.f_base + (int64_t)(k2 >> g.logVP) * a.f_chunk + (pos0 >> flg) * a.f_hi + (pos0 & ((1 << flg) - 1));
@@ -151,16 +159,16 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
     auto issue = [&](int64_t l) {
         const LineAddr b = line_addr(g, kind, l, lgi);
         if constexpr (!INV) {
-            const C *row = in + rowbase(b) + (int64_t)(2 * h) * apos;
-            C *dst = S + n1 * SROW + 2 * h;
-            if (apos == 1) {
+            const C *row = in + rowbase(b);
+            C *dst = S + n1 * srow;
+            if (vcont) {
 #pragma unroll
-                for (int d2 = 0; d2 < 16; d2++) cp_async16(dst + DSTEP * d2, row + DSTEP * d2);
+                for (int d2 = 0; d2 < 16; d2++) cp_async16(dst + lo0 + DSTEP * d2, row + lo0 + DSTEP * d2);
             } else {
 #pragma unroll
                 for (int d2 = 0; d2 < 16; d2++) {
-                    cp_async8(dst + DSTEP * d2, row + (int64_t)DSTEP * d2 * apos);
-                    cp_async8(dst + DSTEP * d2 + 1, row + ((int64_t)DSTEP * d2 + 1) * apos);
+                    cp_async8(dst + lo0 + DSTEP * d2, row + (int64_t)(lo0 + DSTEP * d2) * apos);
+                    cp_async8(dst + lo1 + DSTEP * d2, row + (int64_t)(lo1 + DSTEP * d2) * apos);
                 }
             }
         } else {
@@ -172,8 +180,11 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
     };
 
     int64_t line = blockIdx.x;
+    // prefetch distance: non-persistent, pf_tiles lines (one wave of CTAs); persistent,
+    // pf_tiles iterations of the CTA's own walk
+    const int64_t pfd = PERS ? prm.pf_tiles * lstep : prm.pf_tiles;
     if (PERS && line < nl) issue(line);
-    prefetch(line + (PERS ? lstep : prm.pf_tiles));
+    if (!PERS) prefetch(line + pfd);
     // twiddle tables of this CTA (from the plan's hi/lo table of w_N^m) and the
     // per-thread output twiddle of stage 2, w_N^{d0 ka}
     for (int i = tid; i < KG::NT512 + KG::NT1024; i += KG::NT) {
@@ -189,33 +200,41 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
 
     for (; line < nl; line += lstep) {
         const LineAddr a = line_addr(g, kind, line, lgi);
-        if (PERS) prefetch(line + 2 * lstep);
+        if (PERS && pfd > 0) prefetch(line + pfd);
         if constexpr (!INV) {
             // ---- stage 1: two 16-point transforms over d2
             C x0[16], x1[16];
             if constexpr (PERS) {
                 cp_async_wait_all();
-                const C *src = S + n1 * SROW + 2 * h;
-#pragma unroll
-                for (int d2 = 0; d2 < 16; d2++) {
-                    const float4 v = *reinterpret_cast<const float4 *>(src + DSTEP * d2);
-                    x0[d2] = C{v.x, v.y};
-                    x1[d2] = C{v.z, v.w};
-                }
-            } else {
-                const C *row = in + rowbase(a) + (int64_t)(2 * h) * apos;
-                if (apos == 1) {
+                const C *src = S + n1 * srow;
+                if (vcont) {
 #pragma unroll
                     for (int d2 = 0; d2 < 16; d2++) {
-                        const float4 v = __ldg(reinterpret_cast<const float4 *>(row + DSTEP * d2));
+                        const float4 v = *reinterpret_cast<const float4 *>(src + lo0 + DSTEP * d2);
                         x0[d2] = C{v.x, v.y};
                         x1[d2] = C{v.z, v.w};
                     }
                 } else {
 #pragma unroll
                     for (int d2 = 0; d2 < 16; d2++) {
-                        x0[d2] = ldg(row + (int64_t)DSTEP * d2 * apos);
-                        x1[d2] = ldg(row + ((int64_t)DSTEP * d2 + 1) * apos);
+                        x0[d2] = src[lo0 + DSTEP * d2];
+                        x1[d2] = src[lo1 + DSTEP * d2];
+                    }
+                }
+            } else {
+                const C *row = in + rowbase(a);
+                if (vcont) {
+#pragma unroll
+                    for (int d2 = 0; d2 < 16; d2++) {
+                        const float4 v = __ldg(reinterpret_cast<const float4 *>(row + lo0 + DSTEP * d2));
+                        x0[d2] = C{v.x, v.y};
+                        x1[d2] = C{v.z, v.w};
+                    }
+                } else {
+#pragma unroll
+                    for (int d2 = 0; d2 < 16; d2++) {
+                        x0[d2] = ldg(row + (int64_t)(lo0 + DSTEP * d2) * apos);
+                        x1[d2] = ldg(row + (int64_t)(lo1 + DSTEP * d2) * apos);
                     }
                 }
             }
@@ -224,8 +243,8 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
             __syncthreads();   // tables written; staging fully read
 #pragma unroll
             for (int ka = 0; ka < 16; ka++) {
-                S[KG::s1(ka, d1v, d0v)] = x0[ka];
-                S[KG::s1(ka, d1v + M / 32, d0v)] = x1[ka];
+                S[KG::s1(ka, d1v0, d0v)] = x0[ka];
+                S[KG::s1(ka, d1v1, d0v)] = x1[ka];
             }
             __syncthreads();
             // ---- stage 2: 32-point transforms over d1, unit (d0 = lane, ka = warp)
@@ -291,8 +310,8 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
             C x0[16], x1[16];
 #pragma unroll
             for (int ka = 0; ka < 16; ka++) {
-                x0[ka] = S[KG::s1(ka, d1v, d0v)];
-                x1[ka] = S[KG::s1(ka, d1v + M / 32, d0v)];
+                x0[ka] = S[KG::s1(ka, d1v0, d0v)];
+                x1[ka] = S[KG::s1(ka, d1v1, d0v)];
             }
             if (PERS && line + lstep < nl) {
                 __syncthreads();   // exchange 1 fully read: the region takes the next line
@@ -300,18 +319,18 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
             }
             dft<16, DIR, float>(x0);
             dft<16, DIR, float>(x1);
-            C *row = out + rowbase(a) + (int64_t)(2 * h) * apos;
-            if (apos == 1) {
+            C *row = out + rowbase(a);
+            if (vcont) {
 #pragma unroll
                 for (int d2 = 0; d2 < 16; d2++) {
                     const C u = scale_c(x0[d2]), w = scale_c(x1[d2]);
-                    *reinterpret_cast<float4 *>(row + DSTEP * d2) = float4{u.x, u.y, w.x, w.y};
+                    *reinterpret_cast<float4 *>(row + lo0 + DSTEP * d2) = float4{u.x, u.y, w.x, w.y};
                 }
             } else {
 #pragma unroll
                 for (int d2 = 0; d2 < 16; d2++) {
-                    row[(int64_t)DSTEP * d2 * apos] = scale_c(x0[d2]);
-                    row[((int64_t)DSTEP * d2 + 1) * apos] = scale_c(x1[d2]);
+                    row[(int64_t)(lo0 + DSTEP * d2) * apos] = scale_c(x0[d2]);
+                    row[(int64_t)(lo1 + DSTEP * d2) * apos] = scale_c(x1[d2]);
                 }
             }
         }
@@ -343,7 +362,7 @@ cudaError_t launch_k3(const LineParams &prm, cudaStream_t st) {
     }
     if (prm.g.n != K3Geom::N || prm.g.logVEC != LV || prm.g.logM != LM) return cudaErrorInvalidValue;
     LineParams lp = prm;
-    lp.pf_tiles = resident[dev];
+    lp.pf_tiles = PERS ? 1 : resident[dev];
     const int64_t grid = PERS ? (prm.nlines < resident[dev] ? prm.nlines : resident[dev]) : prm.nlines;
     kern<<<(unsigned)grid, K3Geom::NT, smem, st>>>(lp);
     count_launch();
