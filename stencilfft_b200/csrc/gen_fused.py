@@ -36,11 +36,15 @@ FWD_OOP = {
 }
 # Out-of-place 2D inverse configurations (caller workspace, default variant): y pass
 # variant (frequency side -> work), x pass variant (work -> vector side), log2 of the
-# row interleave.  Measured on B200 at N = 16384, P = 4, B = 64 (c64): y pass on 2-line
-# tiles of a 4-CTA cluster, x pass on the persistent three-stage kernel, 8-row
-# interleave: 3.24 ms against 3.40 for the in-place default.
+# interleave, and "q" for groups of y positions interleaved instead of x-frequency rows
+# (three-stage kernels only).  Measured on B200 at N = 16384, P = 4, B = 64 (c64): both
+# passes on the persistent three-stage kernel, the y pass writing runs of 4 y positions
+# (whole 32-byte sectors), the x pass reading its line 4 elements apart (four lanes per
+# 128-byte line): 1.67 + 1.46 = 3.12 ms per inverse transform, against 3.24 for the
+# row-interleaved intermediate (8-element runs: 1.62 + 1.79; 16-byte runs: partial
+# sectors, 2.2 ms and up for the y pass).
 INV_OOP = {
-    "c64": {(6, 8): (0, 7, 3)},
+    "c64": {(6, 8): (7, 7, 2, "q")},
     "c128": {},
 }
 T = {"c64": "float", "c128": "double"}
@@ -92,11 +96,13 @@ for dt, table in VARIANTS.items():
                         L.append(f"    case ({lv} << 16) | ({lm} << 8) | {vi}: return {g.bit_length() - 1};")
             L += ["    default: return 0;", "    }", "}", ""]
             for name, oop in (("fwd", FWD_OOP), ("inv", INV_OOP)):
-                L += [f"int fused_{name}_oop_{dt}(int logvec, int logm, int *vx, int *vy, int *lg) {{",
+                L += [f"int fused_{name}_oop_{dt}(int logvec, int logm, int *vx, int *vy, int *lg, int *qint) {{",
                       "    switch ((logvec << 8) | logm) {"]
-                for (lv, lm), (v1, v2, lg) in oop[dt].items():
+                for (lv, lm), cfg in oop[dt].items():
+                    v1, v2, lg = cfg[:3]
+                    q = 1 if len(cfg) > 3 and cfg[3] == "q" else 0
                     a, b = (v1, v2) if name == "fwd" else (v2, v1)
-                    L.append(f"    case ({lv} << 8) | {lm}: *vx = {a}; *vy = {b}; *lg = {lg}; return 1;")
+                    L.append(f"    case ({lv} << 8) | {lm}: *vx = {a}; *vy = {b}; *lg = {lg}; *qint = {q}; return 1;")
                 L += ["    default: return 0;", "    }", "}", ""]
         L += ["}  // namespace zm", ""]
         open(f"zm_fft2_{dt}_{d}.cu", "w").write("\n".join(L))

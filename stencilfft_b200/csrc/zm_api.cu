@@ -180,31 +180,33 @@ static LineParams line_params(const zm_plan_s *p, int kind, const void *in, void
 // The out-of-place forward configuration of a 2D plan (x pass in -> work, y pass
 // work -> out, each pass with its own tile shape and a wider row interleave; the
 // in-place y pass rules out interleaves wider than its tile), or false.
-static bool fwd_oop_config(const zm_plan_s *p, int *vx, int *vy, int *lg) {
+static bool fwd_oop_config(const zm_plan_s *p, int *vx, int *vy, int *lg, int *qint) {
     if (p->g.dim != 2 || (p->flags & ZM_FLAG_PERMUTE_ONLY) || p->nvariants == 0 || p->variant != 0) return false;
-    const int ok = p->dtype == ZM_C128 ? zm::fused_fwd_oop_c128(p->g.logVEC, p->g.logM, vx, vy, lg)
-                                       : zm::fused_fwd_oop_c64(p->g.logVEC, p->g.logM, vx, vy, lg);
+    const int ok = p->dtype == ZM_C128 ? zm::fused_fwd_oop_c128(p->g.logVEC, p->g.logM, vx, vy, lg, qint)
+                                       : zm::fused_fwd_oop_c64(p->g.logVEC, p->g.logM, vx, vy, lg, qint);
     if (!ok) return false;
     if (*lg > p->g.logVP) *lg = p->g.logVP;
     return true;
 }
 // The out-of-place inverse configuration of a 2D plan (y pass in -> work, x pass
 // work -> out), or false.
-static bool inv_oop_config(const zm_plan_s *p, int *vx, int *vy, int *lg) {
+static bool inv_oop_config(const zm_plan_s *p, int *vx, int *vy, int *lg, int *qint) {
     if (p->g.dim != 2 || (p->flags & ZM_FLAG_PERMUTE_ONLY) || p->nvariants == 0 || p->variant != 0) return false;
-    const int ok = p->dtype == ZM_C128 ? zm::fused_inv_oop_c128(p->g.logVEC, p->g.logM, vx, vy, lg)
-                                       : zm::fused_inv_oop_c64(p->g.logVEC, p->g.logM, vx, vy, lg);
+    const int ok = p->dtype == ZM_C128 ? zm::fused_inv_oop_c128(p->g.logVEC, p->g.logM, vx, vy, lg, qint)
+                                       : zm::fused_inv_oop_c64(p->g.logVEC, p->g.logM, vx, vy, lg, qint);
     if (!ok) return false;
     if (*lg > p->g.logVP) *lg = p->g.logVP;
     return true;
 }
 
-// `variant` / `lg` >= 0 override the plan's tile shape and row interleave for this pass.
+// `variant` / `lg` >= 0 override the plan's tile shape and row interleave for this pass;
+// `qint` selects the y-position interleave of the intermediate.
 static int run_pass(const zm_plan_s *p, int kind, bool inv, const void *in, void *out, bool scale,
-                    double sre, double sim, cudaStream_t st, int variant = -1, int lg = -1) {
+                    double sre, double sim, cudaStream_t st, int variant = -1, int lg = -1, int qint = 0) {
     LineParams lp = line_params(p, kind, in, out);
     if (variant >= 0) lp.variant = variant;
     if (lg >= 0) lp.lg_inter = lg;
+    lp.inter_q = (qint && lp.lg_inter > 0) ? 1 : 0;
     if (scale) {
         lp.apply_scale = 1;
         lp.scale_re = sre;
@@ -228,13 +230,13 @@ static int forward_impl(zm_plan p, const void *in, void *out, void *work, bool s
     if (!fft_supported(p, &why)) return fail(ZM_ERR_UNSUPPORTED, "%s", why.c_str());
     if (work && (!aligned16(work))) return fail(ZM_ERR_MISALIGNED, "work is not 16-byte aligned");
     if (p->g.dim == 2) {
-        int vx, vy, lg;
-        if (work && fwd_oop_config(p, &vx, &vy, &lg)) {
+        int vx, vy, lg, qi;
+        if (work && fwd_oop_config(p, &vx, &vy, &lg, &qi)) {
             if (overlap(work, in, F) || overlap(work, out, F))
                 return fail(ZM_ERR_INVALID_ARG, "work overlaps in/out");
             // x pass in -> work, y pass work -> out (no in-place constraint on the tile)
-            if ((rc = run_pass(p, zm::PASS_X2, false, in, work, false, 0, 0, st, vx, lg))) return rc;
-            return run_pass(p, zm::PASS_Y2, false, work, out, scale, sre, sim, st, vy, lg);
+            if ((rc = run_pass(p, zm::PASS_X2, false, in, work, false, 0, 0, st, vx, lg, qi))) return rc;
+            return run_pass(p, zm::PASS_Y2, false, work, out, scale, sre, sim, st, vy, lg, qi);
         }
         // x pass: real layout -> REPACK layout (in -> out); y pass in place on out
         if ((rc = run_pass(p, zm::PASS_X2, false, in, out, false, 0, 0, st))) return rc;
@@ -263,10 +265,10 @@ static int inverse_impl(zm_plan p, const void *in, void *out, void *work, double
         return fail(ZM_ERR_INVALID_ARG, "work overlaps in/out");
     void *tmp = work ? work : const_cast<void *>(in);
     if (p->g.dim == 2) {
-        int vx, vy, lg;
-        if (work && inv_oop_config(p, &vx, &vy, &lg)) {
-            if ((rc = run_pass(p, zm::PASS_Y2, true, in, work, false, 0, 0, st, vy, lg))) return rc;
-            return run_pass(p, zm::PASS_X2, true, work, out, true, sre, sim, st, vx, lg);
+        int vx, vy, lg, qi;
+        if (work && inv_oop_config(p, &vx, &vy, &lg, &qi)) {
+            if ((rc = run_pass(p, zm::PASS_Y2, true, in, work, false, 0, 0, st, vy, lg, qi))) return rc;
+            return run_pass(p, zm::PASS_X2, true, work, out, true, sre, sim, st, vx, lg, qi);
         }
         if ((rc = run_pass(p, zm::PASS_Y2, true, in, tmp, false, 0, 0, st))) return rc;
         return run_pass(p, zm::PASS_X2, true, tmp, out, true, sre, sim, st);

@@ -84,7 +84,7 @@ cudaError_t launch_line_pass(const LineParams &prm, int dtype, bool inv, cudaStr
         if (handled) return e;
     }
     // the runtime-sized kernel reads and writes only the plain REPACK intermediate
-    if (prm.lg_inter != 0) return cudaErrorInvalidValue;
+    if (prm.lg_inter != 0 || prm.inter_q) return cudaErrorInvalidValue;
     const int ept = ept_for(dtype);
     const int threads = (int)((prm.T * prm.g.n) / ept);
     const size_t smem = (size_t)prm.T * prm.g.n * (dtype == 0 ? 16 : 8);

@@ -811,6 +811,7 @@ cudaError_t launch_fused(const LineParams &prm, cudaStream_t st) {
     constexpr size_t smem = fused_smem_bytes<T, LV, LM, CL, TL, NT, INV, PERS>();
     static_assert(smem <= 227 * 1024, "shared memory of one CTA");
     constexpr bool persistent = fused_persistent<T, LV, LM, CL, TL, NT, INV, PERS>();
+    if (prm.inter_q) return cudaErrorInvalidValue;   // row-interleaved intermediates only
     // the staging rows of a persistent pass hold sg = 1, 2 or 4 interleaved lines and
     // are sized for sg <= TL: a wider interleave of the y pass's vector side is refused
     if (persistent && prm.kind == PASS_Y2 && prm.lg_inter > 0 &&

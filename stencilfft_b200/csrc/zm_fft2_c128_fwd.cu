@@ -59,13 +59,13 @@ int fused_interleave_lg_c128(int logvec, int logm, int variant) {
     }
 }
 
-int fused_fwd_oop_c128(int logvec, int logm, int *vx, int *vy, int *lg) {
+int fused_fwd_oop_c128(int logvec, int logm, int *vx, int *vy, int *lg, int *qint) {
     switch ((logvec << 8) | logm) {
     default: return 0;
     }
 }
 
-int fused_inv_oop_c128(int logvec, int logm, int *vx, int *vy, int *lg) {
+int fused_inv_oop_c128(int logvec, int logm, int *vx, int *vy, int *lg, int *qint) {
     switch ((logvec << 8) | logm) {
     default: return 0;
     }

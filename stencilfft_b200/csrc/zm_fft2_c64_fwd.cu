@@ -88,18 +88,18 @@ int fused_interleave_lg_c64(int logvec, int logm, int variant) {
     }
 }
 
-int fused_fwd_oop_c64(int logvec, int logm, int *vx, int *vy, int *lg) {
+int fused_fwd_oop_c64(int logvec, int logm, int *vx, int *vy, int *lg, int *qint) {
     switch ((logvec << 8) | logm) {
-    case (6 << 8) | 8: *vx = 7; *vy = 6; *lg = 3; return 1;
-    case (5 << 8) | 8: *vx = 5; *vy = 5; *lg = 1; return 1;
-    case (6 << 8) | 7: *vx = 2; *vy = 2; *lg = 1; return 1;
+    case (6 << 8) | 8: *vx = 7; *vy = 6; *lg = 3; *qint = 0; return 1;
+    case (5 << 8) | 8: *vx = 5; *vy = 5; *lg = 1; *qint = 0; return 1;
+    case (6 << 8) | 7: *vx = 2; *vy = 2; *lg = 1; *qint = 0; return 1;
     default: return 0;
     }
 }
 
-int fused_inv_oop_c64(int logvec, int logm, int *vx, int *vy, int *lg) {
+int fused_inv_oop_c64(int logvec, int logm, int *vx, int *vy, int *lg, int *qint) {
     switch ((logvec << 8) | logm) {
-    case (6 << 8) | 8: *vx = 7; *vy = 0; *lg = 3; return 1;
+    case (6 << 8) | 8: *vx = 7; *vy = 7; *lg = 2; *qint = 1; return 1;
     default: return 0;
     }
 }

@@ -75,7 +75,10 @@ ZM_DEV void prefetch_l2_bytes(const void *p, int64_t bytes) {
 // (stage-A) reads want: vector-side rows of VEC + 4 elements (conflict-free 16-byte
 // reads of 16 rows per warp), or the frequency side as [kc][k mod 512].  Each thread
 // reads back only what it copied itself.  The twiddle tables are filled once per CTA.
-template <int LV, int LM, bool INV, bool PERS>
+// VM, the vector side's address form: 0 contiguous (a_pos = 1), 1 a stride (the row
+// interleave of the intermediate, a_pos = G), 2 runs of 2^a_lg positions a_hi apart (the
+// y-position interleave).
+template <int LV, int LM, bool INV, bool PERS, int VM>
 __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
     static_assert(LV + LM == 14, "lines of 2^14 points");
     static_assert(LM >= 5 && LM <= 9 && LV <= 9, "vector / column split of the line");
@@ -108,9 +111,17 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
     // intermediate): lanes h = 0, 1 take adjacent positions, so the 32 lanes of a load
     // touch 16 cache lines instead of 32.
     const int h = tid % HP, n1 = tid / HP;
-    const LineAddr a0 = line_addr(g, kind, 0, lgi);
-    const int64_t apos = a0.a_pos;
-    const bool vcont = apos == 1;
+    const bool qint = prm.inter_q != 0;
+    const LineAddr a0 = line_addr(g, kind, 0, lgi, qint);
+    // vector-side offset of position n2 within a row
+    const int alg = VM == 2 ? a0.a_lg : 0;
+    const int64_t ahi = VM == 0 ? 1 : a0.a_hi;
+    auto voff = [&](int n2) -> int64_t {
+        if constexpr (VM == 0) return n2;
+        else if constexpr (VM == 1) return (int64_t)n2 * ahi;
+        else return (int64_t)(n2 >> alg) * ahi + (n2 & ((1 << alg) - 1));
+    };
+    constexpr bool vcont = VM != 1;   // positions n2, n2 + 1 (n2 even) adjacent
     const int lo0 = vcont ? 2 * h : h, lo1 = vcont ? 2 * h + 1 : h + HP;
     const int d0v = n1 & 31;
     const int d1v0 = (n1 >> 5) + (M / 32) * lo0, d1v1 = (n1 >> 5) + (M / 32) * lo1;
@@ -125,7 +136,7 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
     // vector side: row base of n1 in line a (positions n2 of the row are a_pos apart)
     auto rowbase = [&](const LineAddr &a) {
         const int64_t r = (int64_t)n1 << LV;
-        return a.a_base + (r >> g.logL) * a.a_chunk + (r & (g.L - 1)) * a.a_pos;
+        return a.a_base + (r >> g.logL) * a.a_chunk + ((r & (g.L - 1)) >> alg) * ahi;
     };
     // frequency side: element k = tid + 512 kc of line a is at fofs(a) + kc * fstep
     const int k2 = tid & (VEC - 1);
@@ -147,28 +158,32 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
         if (l >= nl) return;
         const int nch = (int)(g.n >> g.logL);
         if (tid >= nch) return;
-        const LineAddr fa = line_addr(g, kind, l, lgi);
+        const LineAddr fa = line_addr(g, kind, l, lgi, qint);
         if (!INV) {
-            if (apos == 1 || (l & (apos - 1)) == 0)
-                prefetch_l2_bytes(in + fa.a_base + tid * fa.a_chunk, g.L * fa.a_pos * (int64_t)sizeof(C));
+            if (VM == 0 || (VM == 1 && (l & (ahi - 1)) == 0))
+                prefetch_l2_bytes(in + fa.a_base + tid * fa.a_chunk, g.L * ahi * (int64_t)sizeof(C));
         } else if (fa.f_hi == 1) {
             prefetch_l2_bytes(in + fa.f_base + tid * fa.f_chunk, g.L * (int64_t)sizeof(C));
+        } else if (qint && fa.f_lg == 0 && (l & (fa.f_hi - 1)) == 0) {
+            // x pass on a y-position-interleaved intermediate: the first line of a group
+            // fetches the group's G L contiguous elements of each chunk
+            prefetch_l2_bytes(in + fa.f_base + tid * fa.f_chunk, g.L * fa.f_hi * (int64_t)sizeof(C));
         }
     };
     // asynchronous copies of line l's input into the staging region (PERS)
     auto issue = [&](int64_t l) {
-        const LineAddr b = line_addr(g, kind, l, lgi);
+        const LineAddr b = line_addr(g, kind, l, lgi, qint);
         if constexpr (!INV) {
             const C *row = in + rowbase(b);
             C *dst = S + n1 * srow;
-            if (vcont) {
+            if constexpr (vcont) {
 #pragma unroll
-                for (int d2 = 0; d2 < 16; d2++) cp_async16(dst + lo0 + DSTEP * d2, row + lo0 + DSTEP * d2);
+                for (int d2 = 0; d2 < 16; d2++) cp_async16(dst + lo0 + DSTEP * d2, row + voff(lo0 + DSTEP * d2));
             } else {
 #pragma unroll
                 for (int d2 = 0; d2 < 16; d2++) {
-                    cp_async8(dst + lo0 + DSTEP * d2, row + (int64_t)(lo0 + DSTEP * d2) * apos);
-                    cp_async8(dst + lo1 + DSTEP * d2, row + (int64_t)(lo1 + DSTEP * d2) * apos);
+                    cp_async8(dst + lo0 + DSTEP * d2, row + voff(lo0 + DSTEP * d2));
+                    cp_async8(dst + lo1 + DSTEP * d2, row + voff(lo1 + DSTEP * d2));
                 }
             }
         } else {
@@ -199,7 +214,7 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
     const Wt f1 = ldtw(twn, lane * ka2);
 
     for (; line < nl; line += lstep) {
-        const LineAddr a = line_addr(g, kind, line, lgi);
+        const LineAddr a = line_addr(g, kind, line, lgi, qint);
         if (PERS && pfd > 0) prefetch(line + pfd);
         if constexpr (!INV) {
             // ---- stage 1: two 16-point transforms over d2
@@ -207,7 +222,7 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
             if constexpr (PERS) {
                 cp_async_wait_all();
                 const C *src = S + n1 * srow;
-                if (vcont) {
+                if constexpr (vcont) {
 #pragma unroll
                     for (int d2 = 0; d2 < 16; d2++) {
                         const float4 v = *reinterpret_cast<const float4 *>(src + lo0 + DSTEP * d2);
@@ -223,18 +238,18 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
                 }
             } else {
                 const C *row = in + rowbase(a);
-                if (vcont) {
+                if constexpr (vcont) {
 #pragma unroll
                     for (int d2 = 0; d2 < 16; d2++) {
-                        const float4 v = __ldg(reinterpret_cast<const float4 *>(row + lo0 + DSTEP * d2));
+                        const float4 v = __ldg(reinterpret_cast<const float4 *>(row + voff(lo0 + DSTEP * d2)));
                         x0[d2] = C{v.x, v.y};
                         x1[d2] = C{v.z, v.w};
                     }
                 } else {
 #pragma unroll
                     for (int d2 = 0; d2 < 16; d2++) {
-                        x0[d2] = ldg(row + (int64_t)(lo0 + DSTEP * d2) * apos);
-                        x1[d2] = ldg(row + (int64_t)(lo1 + DSTEP * d2) * apos);
+                        x0[d2] = ldg(row + voff(lo0 + DSTEP * d2));
+                        x1[d2] = ldg(row + voff(lo1 + DSTEP * d2));
                     }
                 }
             }
@@ -320,17 +335,17 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
             dft<16, DIR, float>(x0);
             dft<16, DIR, float>(x1);
             C *row = out + rowbase(a);
-            if (vcont) {
+            if constexpr (vcont) {
 #pragma unroll
                 for (int d2 = 0; d2 < 16; d2++) {
                     const C u = scale_c(x0[d2]), w = scale_c(x1[d2]);
-                    *reinterpret_cast<float4 *>(row + lo0 + DSTEP * d2) = float4{u.x, u.y, w.x, w.y};
+                    *reinterpret_cast<float4 *>(row + voff(lo0 + DSTEP * d2)) = float4{u.x, u.y, w.x, w.y};
                 }
             } else {
 #pragma unroll
                 for (int d2 = 0; d2 < 16; d2++) {
-                    row[(int64_t)(lo0 + DSTEP * d2) * apos] = scale_c(x0[d2]);
-                    row[(int64_t)(lo1 + DSTEP * d2) * apos] = scale_c(x1[d2]);
+                    row[voff(lo0 + DSTEP * d2)] = scale_c(x0[d2]);
+                    row[voff(lo1 + DSTEP * d2)] = scale_c(x1[d2]);
                 }
             }
         }
@@ -338,12 +353,12 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
 }
 
 // Non-persistent: one CTA per line, L2 prefetch one wave of CTAs ahead.  PERS: one CTA
-// per SM (or fewer when there are fewer lines).
-template <int LV, int LM, bool INV, bool PERS = false>
-cudaError_t launch_k3(const LineParams &prm, cudaStream_t st) {
+// per SM (or fewer when there are fewer lines), L2 prefetch one line of its walk ahead.
+template <int LV, int LM, bool INV, bool PERS, int VM>
+cudaError_t launch_k3_vm(const LineParams &prm, cudaStream_t st) {
     constexpr size_t smem = K3Geom::SMEM;
     static_assert(smem <= 227 * 1024, "shared memory of one CTA");
-    auto kern = k3_pass_kernel<LV, LM, INV, PERS>;
+    auto kern = k3_pass_kernel<LV, LM, INV, PERS, VM>;
     static int attr_done[64], resident[64];
     int dev = 0;
     cudaGetDevice(&dev);
@@ -360,13 +375,23 @@ cudaError_t launch_k3(const LineParams &prm, cudaStream_t st) {
         resident[dev] = per_sm * sms;
         attr_done[dev] = 1;
     }
-    if (prm.g.n != K3Geom::N || prm.g.logVEC != LV || prm.g.logM != LM) return cudaErrorInvalidValue;
     LineParams lp = prm;
     lp.pf_tiles = PERS ? 1 : resident[dev];
     const int64_t grid = PERS ? (prm.nlines < resident[dev] ? prm.nlines : resident[dev]) : prm.nlines;
     kern<<<(unsigned)grid, K3Geom::NT, smem, st>>>(lp);
     count_launch();
     return cudaGetLastError();
+}
+
+// 2D passes of N = 2^14 lines only; the vector side's address form follows from the pass
+// kind and the intermediate's interleave.
+template <int LV, int LM, bool INV, bool PERS = false>
+cudaError_t launch_k3(const LineParams &prm, cudaStream_t st) {
+    if (prm.g.n != K3Geom::N || prm.g.logVEC != LV || prm.g.logM != LM || prm.g.dim != 2) return cudaErrorInvalidValue;
+    if (prm.kind == PASS_Y2 && prm.lg_inter > 0)
+        return prm.inter_q ? launch_k3_vm<LV, LM, INV, PERS, 2>(prm, st) : launch_k3_vm<LV, LM, INV, PERS, 1>(prm, st);
+    if (prm.kind != PASS_X2 && prm.kind != PASS_Y2) return cudaErrorInvalidValue;
+    return launch_k3_vm<LV, LM, INV, PERS, 0>(prm, st);
 }
 
 }  // namespace zm

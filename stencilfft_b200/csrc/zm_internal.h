@@ -32,13 +32,13 @@ int fused_variants_c128(int logvec, int logm);
 // supports (0 = none).
 int fused_interleave_lg_c64(int logvec, int logm, int variant);
 int fused_interleave_lg_c128(int logvec, int logm, int variant);
-// 1 and the (x variant, y variant, log2 interleave) of the out-of-place 2D forward
-// configuration of (VEC, M), when there is one.
-int fused_fwd_oop_c64(int logvec, int logm, int *vx, int *vy, int *lg);
-int fused_fwd_oop_c128(int logvec, int logm, int *vx, int *vy, int *lg);
+// 1 and the (x variant, y variant, log2 interleave, y-position interleave flag) of the
+// out-of-place 2D forward configuration of (VEC, M), when there is one.
+int fused_fwd_oop_c64(int logvec, int logm, int *vx, int *vy, int *lg, int *qint);
+int fused_fwd_oop_c128(int logvec, int logm, int *vx, int *vy, int *lg, int *qint);
 // the same for the out-of-place 2D inverse (y pass in -> work, x pass work -> out)
-int fused_inv_oop_c64(int logvec, int logm, int *vx, int *vy, int *lg);
-int fused_inv_oop_c128(int logvec, int logm, int *vx, int *vy, int *lg);
+int fused_inv_oop_c64(int logvec, int logm, int *vx, int *vy, int *lg, int *qint);
+int fused_inv_oop_c128(int logvec, int logm, int *vx, int *vy, int *lg, int *qint);
 
 // zm_stencil.cu
 enum StencilOp : int { ST_LAPLACE = 0, ST_DX = 1, ST_DY = 2, ST_ALL = 3 };

@@ -40,6 +40,8 @@ struct LineParams {
     int variant;       // tile-shape variant of the size-specialised kernel (0 = default)
     int permute_only;  // skip all arithmetic (reference do_compute=false)
     int lg_inter;      // 2D: log2 of the row interleave of the x -> y intermediate (0 = plain REPACK layout)
+    int inter_q;       // 2D, lg_inter > 0: interleave groups of 2^lg_inter y positions instead of
+                       // x-frequency rows (three-stage passes only)
     int *err;          // device word set to 1 when a bounded wait inside a kernel gives up
     int64_t pf_tiles;  // size-specialised passes: L2 prefetch distance in tiles (0 = none)
     // radix schedules of the two sub-transforms (first stage first)
