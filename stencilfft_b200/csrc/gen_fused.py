@@ -3,7 +3,7 @@ dispatch tables.  Each (log2 VEC, log2 M) pair lists variants (cluster size CL, 
 per tile TL, threads NT[, "p" = persistent forward pass with bulk-copy prefetch]); the
 plan's `variant` picks one; "k3" marks the three-stage 512-thread pass of zm_fft3.cuh
 for complex64 lines of 2^14 points ("k3p": its persistent form with asynchronous copies
-of the next line).  Variant 0, the default, is
+of the next line; "k3c": the forward y pass on buddy-line CTA pairs).  Variant 0, the default, is
 the fastest one measured on B200 at the sizes the table was tuned on; zm_plan_autotune
 re-measures them for a plan."""
 VARIANTS = {
@@ -15,7 +15,7 @@ VARIANTS = {
         (5, 8): [(2, 2, 512), (1, 1, 512), (2, 1, 256), (4, 4, 512), (2, 4, 1024), (1, 2, 1024)],
         (6, 7): [(2, 2, 512), (1, 1, 512), (1, 2, 1024)],
         (6, 8): [(4, 2, 512), (2, 1, 512), (1, 1, 1024), (8, 4, 512), (4, 4, 1024), (4, 2, 512, "p"),
-                 (1, 1, 512, "k3"), (1, 1, 512, "k3p")],
+                 (1, 1, 512, "k3"), (1, 1, 512, "k3p"), (1, 1, 512, "k3c")],
     },
     "c128": {
         (4, 4): [(1, 16, 256)], (4, 5): [(1, 8, 256)], (4, 6): [(1, 4, 256)], (2, 7): [(1, 8, 256), (1, 4, 128), (1, 16, 512)],
@@ -27,11 +27,11 @@ VARIANTS = {
 # Out-of-place 2D forward configurations (used when the caller passes a workspace and the
 # plan runs its default variant): x pass variant, y pass variant, log2 of the row
 # interleave of the intermediate.  Measured on B200 at N = 16384, P = 4, B = 64 (c64):
-# x pass on the persistent three-stage kernel (1.28 ms), y pass on the one-line-per-CTA
-# three-stage kernel reading the 8-row interleave (1.75 ms): 3.03 ms per forward
-# transform against 4.61 for the in-place default.
+# x pass on the persistent three-stage kernel (1.21 ms), y pass on buddy-line CTA pairs
+# of the three-stage kernel reading the 8-row interleave (1.77 ms; one line per CTA
+# 1.81): 2.97 ms per forward transform against 4.61 for the in-place default.
 FWD_OOP = {
-    "c64": {(6, 8): (7, 6, 3), (5, 8): (5, 5, 1), (6, 7): (2, 2, 1)},
+    "c64": {(6, 8): (7, 8, 3), (5, 8): (5, 5, 1), (6, 7): (2, 2, 1)},
     "c128": {},
 }
 # Out-of-place 2D inverse configurations (caller workspace, default variant): y pass
@@ -63,10 +63,11 @@ for dt, table in VARIANTS.items():
             for vi, v in enumerate(vs):
                 cl, tl, nt = v[:3]
                 pers = "true" if len(v) > 3 and v[3] == "p" else "false"
-                if len(v) > 3 and v[3] in ("k3", "k3p"):
+                if len(v) > 3 and v[3] in ("k3", "k3p", "k3c"):
                     L.append(f"    case ({lv} << 16) | ({lm} << 8) | {vi}: "
                              f"return launch_k3<{lv}, {lm}, {'true' if inv else 'false'}, "
-                             f"{'true' if v[3] == 'k3p' else 'false'}>(prm, st);")
+                             f"{'true' if v[3] == 'k3p' else 'false'}, "
+                             f"{'true' if v[3] == 'k3c' else 'false'}>(prm, st);")
                     continue
                 L.append(f"    case ({lv} << 16) | ({lm} << 8) | {vi}: "
                          f"return launch_fused<{T[dt]}, {lv}, {lm}, {cl}, {tl}, {nt}, {'true' if inv else 'false'}, {pers}>(prm, st);")

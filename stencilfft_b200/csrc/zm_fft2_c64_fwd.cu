@@ -43,8 +43,9 @@ cudaError_t launch_fused_c64_fwd(const LineParams &prm, cudaStream_t st, bool *h
     case (6 << 16) | (8 << 8) | 3: return launch_fused<float, 6, 8, 8, 4, 512, false, false>(prm, st);
     case (6 << 16) | (8 << 8) | 4: return launch_fused<float, 6, 8, 4, 4, 1024, false, false>(prm, st);
     case (6 << 16) | (8 << 8) | 5: return launch_fused<float, 6, 8, 4, 2, 512, false, true>(prm, st);
-    case (6 << 16) | (8 << 8) | 6: return launch_k3<6, 8, false, false>(prm, st);
-    case (6 << 16) | (8 << 8) | 7: return launch_k3<6, 8, false, true>(prm, st);
+    case (6 << 16) | (8 << 8) | 6: return launch_k3<6, 8, false, false, false>(prm, st);
+    case (6 << 16) | (8 << 8) | 7: return launch_k3<6, 8, false, true, false>(prm, st);
+    case (6 << 16) | (8 << 8) | 8: return launch_k3<6, 8, false, false, true>(prm, st);
     default: break;
     }
     *handled = false;
@@ -62,7 +63,7 @@ int fused_variants_c64(int logvec, int logm) {
     case (4 << 8) | 8: return 4;
     case (5 << 8) | 8: return 6;
     case (6 << 8) | 7: return 3;
-    case (6 << 8) | 8: return 8;
+    case (6 << 8) | 8: return 9;
     default: return 0;
     }
 }
@@ -90,7 +91,7 @@ int fused_interleave_lg_c64(int logvec, int logm, int variant) {
 
 int fused_fwd_oop_c64(int logvec, int logm, int *vx, int *vy, int *lg, int *qint) {
     switch ((logvec << 8) | logm) {
-    case (6 << 8) | 8: *vx = 7; *vy = 6; *lg = 3; *qint = 0; return 1;
+    case (6 << 8) | 8: *vx = 7; *vy = 8; *lg = 3; *qint = 0; return 1;
     case (5 << 8) | 8: *vx = 5; *vy = 5; *lg = 1; *qint = 0; return 1;
     case (6 << 8) | 7: *vx = 2; *vy = 2; *lg = 1; *qint = 0; return 1;
     default: return 0;

@@ -43,8 +43,9 @@ cudaError_t launch_fused_c64_inv(const LineParams &prm, cudaStream_t st, bool *h
     case (6 << 16) | (8 << 8) | 3: return launch_fused<float, 6, 8, 8, 4, 512, true, false>(prm, st);
     case (6 << 16) | (8 << 8) | 4: return launch_fused<float, 6, 8, 4, 4, 1024, true, false>(prm, st);
     case (6 << 16) | (8 << 8) | 5: return launch_fused<float, 6, 8, 4, 2, 512, true, true>(prm, st);
-    case (6 << 16) | (8 << 8) | 6: return launch_k3<6, 8, true, false>(prm, st);
-    case (6 << 16) | (8 << 8) | 7: return launch_k3<6, 8, true, true>(prm, st);
+    case (6 << 16) | (8 << 8) | 6: return launch_k3<6, 8, true, false, false>(prm, st);
+    case (6 << 16) | (8 << 8) | 7: return launch_k3<6, 8, true, true, false>(prm, st);
+    case (6 << 16) | (8 << 8) | 8: return launch_k3<6, 8, true, false, true>(prm, st);
     default: break;
     }
     *handled = false;

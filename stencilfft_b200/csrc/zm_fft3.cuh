@@ -30,6 +30,8 @@
 // threads, one CTA per SM (the line and the tables fill 160 KB of shared memory).
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "zm_common.cuh"
 #include "zm_lines.cuh"
 
@@ -78,7 +80,12 @@ ZM_DEV void prefetch_l2_bytes(const void *p, int64_t bytes) {
 // VM, the vector side's address form: 0 contiguous (a_pos = 1), 1 a stride (the row
 // interleave of the intermediate, a_pos = G), 2 runs of 2^a_lg positions a_hi apart (the
 // y-position interleave).
-template <int LV, int LM, bool INV, bool PERS, int VM>
+// PAIR (forward, VM = 1, one line per CTA): clusters of two CTAs on the buddy lines 2i,
+// 2i + 1, whose elements share every 16-byte pair of the row interleave.  Each CTA loads
+// the pairs of one of its two stage-1 units for both lines, keeps its own element and
+// stores its partner's into the partner's shared memory (distributed shared memory), so
+// a line's strided reads need half the L2 sector requests.
+template <int LV, int LM, bool INV, bool PERS, int VM, bool PAIR = false>
 __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
     static_assert(LV + LM == 14, "lines of 2^14 points");
     static_assert(LM >= 5 && LM <= 9 && LV <= 9, "vector / column split of the line");
@@ -195,6 +202,8 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
     };
 
     int64_t line = blockIdx.x;
+    if constexpr (PAIR && !INV && !PERS && VM == 1)   // matched by the wait before the first remote store
+        asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
     // prefetch distance: non-persistent, pf_tiles lines (one wave of CTAs); persistent,
     // pf_tiles iterations of the CTA's own walk
     const int64_t pfd = PERS ? prm.pf_tiles * lstep : prm.pf_tiles;
@@ -244,6 +253,32 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
                         const float4 v = __ldg(reinterpret_cast<const float4 *>(row + voff(lo0 + DSTEP * d2)));
                         x0[d2] = C{v.x, v.y};
                         x1[d2] = C{v.z, v.w};
+                    }
+                } else if constexpr (PAIR && VM == 1) {
+                    // rank rk (= line & 1) loads unit b = rk of both buddy lines; the
+                    // partner's element goes to slot d2 * 512 + tid of its shared memory
+                    namespace cg = cooperative_groups;
+                    const int rk = (int)cg::this_cluster().block_rank();
+                    C *peer = cg::this_cluster().map_shared_rank(S, rk ^ 1);
+                    const C *prow = row - (line & 1);
+                    const int lob = rk ? lo1 : lo0;
+                    float4 v[16];
+#pragma unroll
+                    for (int d2 = 0; d2 < 16; d2++)
+                        v[d2] = __ldg(reinterpret_cast<const float4 *>(prow + voff(lob + DSTEP * d2)));
+                    asm volatile("barrier.cluster.wait.aligned;" ::: "memory");   // partner running
+#pragma unroll
+                    for (int d2 = 0; d2 < 16; d2++) {
+                        const C e0{v[d2].x, v[d2].y}, e1{v[d2].z, v[d2].w};
+                        peer[d2 * 512 + tid] = rk ? e0 : e1;
+                        if (rk) x1[d2] = e1;
+                        else x0[d2] = e0;
+                    }
+                    cg::this_cluster().sync();   // both halves delivered
+#pragma unroll
+                    for (int d2 = 0; d2 < 16; d2++) {
+                        if (rk) x0[d2] = S[d2 * 512 + tid];
+                        else x1[d2] = S[d2 * 512 + tid];
                     }
                 } else {
 #pragma unroll
@@ -354,11 +389,12 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
 
 // Non-persistent: one CTA per line, L2 prefetch one wave of CTAs ahead.  PERS: one CTA
 // per SM (or fewer when there are fewer lines), L2 prefetch one line of its walk ahead.
-template <int LV, int LM, bool INV, bool PERS, int VM>
+template <int LV, int LM, bool INV, bool PERS, int VM, bool PAIR = false>
 cudaError_t launch_k3_vm(const LineParams &prm, cudaStream_t st) {
     constexpr size_t smem = K3Geom::SMEM;
     static_assert(smem <= 227 * 1024, "shared memory of one CTA");
-    auto kern = k3_pass_kernel<LV, LM, INV, PERS, VM>;
+    static_assert(!PAIR || (!PERS && !INV && VM == 1), "buddy-line pairs: forward strided one-line passes");
+    auto kern = k3_pass_kernel<LV, LM, INV, PERS, VM, PAIR>;
     static int attr_done[64], resident[64];
     int dev = 0;
     cudaGetDevice(&dev);
@@ -378,16 +414,39 @@ cudaError_t launch_k3_vm(const LineParams &prm, cudaStream_t st) {
     LineParams lp = prm;
     lp.pf_tiles = PERS ? 1 : resident[dev];
     const int64_t grid = PERS ? (prm.nlines < resident[dev] ? prm.nlines : resident[dev]) : prm.nlines;
-    kern<<<(unsigned)grid, K3Geom::NT, smem, st>>>(lp);
+    if constexpr (PAIR) {
+        if ((grid & 1) || prm.lg_inter < 1) return cudaErrorInvalidValue;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)grid);
+        cfg.blockDim = dim3(K3Geom::NT);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaError_t e = cudaLaunchKernelEx(&cfg, kern, lp);
+        if (e != cudaSuccess) return e;
+    } else {
+        kern<<<(unsigned)grid, K3Geom::NT, smem, st>>>(lp);
+    }
     count_launch();
     return cudaGetLastError();
 }
 
 // 2D passes of N = 2^14 lines only; the vector side's address form follows from the pass
 // kind and the intermediate's interleave.
-template <int LV, int LM, bool INV, bool PERS = false>
+// PAIR: the forward y pass on a row-interleaved intermediate runs on buddy-line pairs;
+// every other pass of the variant runs the one-line kernel.
+template <int LV, int LM, bool INV, bool PERS = false, bool PAIR = false>
 cudaError_t launch_k3(const LineParams &prm, cudaStream_t st) {
     if (prm.g.n != K3Geom::N || prm.g.logVEC != LV || prm.g.logM != LM || prm.g.dim != 2) return cudaErrorInvalidValue;
+    if constexpr (PAIR && !INV && !PERS)
+        if (prm.kind == PASS_Y2 && prm.lg_inter > 0 && !prm.inter_q)
+            return launch_k3_vm<LV, LM, INV, PERS, 1, true>(prm, st);
     if (prm.kind == PASS_Y2 && prm.lg_inter > 0)
         return prm.inter_q ? launch_k3_vm<LV, LM, INV, PERS, 2>(prm, st) : launch_k3_vm<LV, LM, INV, PERS, 1>(prm, st);
     if (prm.kind != PASS_X2 && prm.kind != PASS_Y2) return cudaErrorInvalidValue;
