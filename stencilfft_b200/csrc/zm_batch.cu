@@ -134,6 +134,33 @@ ZM_DEV int64_t real_elem(int64_t gr, int64_t gc, const Geom &g) {
     return (((rid << g.logP) + cid) << (2 * g.logL)) + (lr << g.logL) + pos;
 }
 
+// Both sub-transforms of a tile: compile-time-sized stages for the complex64 tiles with
+// VEC = 4 (the layout the B autotuner picks for the batch sizes, B = N / 8 at P = 2) and
+// M = 16 .. 1024; the runtime-sized stages for every other shape.
+template <typename T, int EPT, bool INV, int LM>
+__device__ __noinline__ void tile_transform_v4(cpx<T> *s, int tid, const tw<T> *twN) {
+    tile_transform_ct<T, EPT, INV, 2, LM, kBatchThreads>(s, tid, twN);
+}
+template <typename T, int EPT, bool INV>
+ZM_DEV void batch_tile_transform(cpx<T> *s, const BatchField &f, int nthr, int tid, const tw<T> *twN) {
+    const Geom &g = f.g;
+    if constexpr (sizeof(T) == 4 && EPT == 16) {
+        if (g.logVEC == 2) {
+            switch (g.logM) {
+            case 4: return tile_transform_v4<T, EPT, INV, 4>(s, tid, twN);
+            case 5: return tile_transform_v4<T, EPT, INV, 5>(s, tid, twN);
+            case 6: return tile_transform_v4<T, EPT, INV, 6>(s, tid, twN);
+            case 7: return tile_transform_v4<T, EPT, INV, 7>(s, tid, twN);
+            case 8: return tile_transform_v4<T, EPT, INV, 8>(s, tid, twN);
+            case 9: return tile_transform_v4<T, EPT, INV, 9>(s, tid, twN);
+            case 10: return tile_transform_v4<T, EPT, INV, 10>(s, tid, twN);
+            default: break;
+            }
+        }
+    }
+    tile_transform<T, EPT, INV>(s, g, f.rad_vec, f.nst_vec, f.rad_m, f.nst_m, nthr, tid, twN);
+}
+
 template <typename T, int EPT>
 __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(const BatchParams bp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -208,19 +235,19 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(const BatchPara
             if (S.op == BOP_X_FWD || S.op == BOP_Y_FWD) {
                 tile_load_vec(c, g, s, in, nthr, tid);
                 __syncthreads();
-                tile_transform<T, EPT, false>(s, g, sf.rad_vec, sf.nst_vec, sf.rad_m, sf.nst_m, nthr, tid, twN);
+                batch_tile_transform<T, EPT, false>(s, sf, nthr, tid, twN);
                 tile_store_freq(c, g, s, out, false, (T)1, (T)0, nthr, tid);
             } else if (S.op == BOP_X_INV || S.op == BOP_Y_INV) {
                 tile_load_freq(c, g, s, in, nthr, tid);
                 __syncthreads();
-                tile_transform<T, EPT, true>(s, g, sf.rad_vec, sf.nst_vec, sf.rad_m, sf.nst_m, nthr, tid, twN);
+                batch_tile_transform<T, EPT, true>(s, sf, nthr, tid, twN);
                 const bool scl = S.scale && xpass;
                 const T sc = (T)(1.0 / ((double)g.n * (double)g.n));
                 tile_store_vec(c, g, s, out, scl, sc, (T)0, nthr, tid);
             } else {   // BOP_Y_POISSON
                 tile_load_vec(c, g, s, in, nthr, tid);
                 __syncthreads();
-                tile_transform<T, EPT, false>(s, g, sf.rad_vec, sf.nst_vec, sf.rad_m, sf.nst_m, nthr, tid, twN);
+                batch_tile_transform<T, EPT, false>(s, sf, nthr, tid, twN);
                 // slot (t, k1, k2) holds the frequency the y pass would store at rank
                 // (rid = k2 / VP, cid), local row p, column pos = k1 VP + k2 % VP
                 // (reciprocal_to_global, utils.h:265-268)
@@ -240,7 +267,7 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(const BatchPara
                     s[e] = {(T)(v.x * fac), (T)(v.y * fac)};
                 }
                 __syncthreads();
-                tile_transform<T, EPT, true>(s, g, sf.rad_vec, sf.nst_vec, sf.rad_m, sf.nst_m, nthr, tid, twN);
+                batch_tile_transform<T, EPT, true>(s, sf, nthr, tid, twN);
                 tile_store_vec(c, g, s, out, false, (T)1, (T)0, nthr, tid);
             }
         }

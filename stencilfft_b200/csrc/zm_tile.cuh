@@ -112,6 +112,98 @@ ZM_DEV void tile_transform(cpx<T> *s, const Geom &g, const int *rad_vec, int nst
     }
 }
 
+// ------------------------------------------------ compile-time-sized sub-transforms
+// The same Stockham stages as stockham_stage / run_subfft / tile_transform, with the
+// tile's VEC = 2^LV and M = 2^LM, the thread count NT and the radix schedule (remainder
+// radix first, then radix 2^RL stages, as radix_schedule) fixed at compile time, so the
+// per-point index arithmetic folds to constants.  Same shared-memory layout, same
+// arithmetic in the same order.
+constexpr int ct_log2(int x) { return x <= 1 ? 0 : 1 + ct_log2(x >> 1); }
+
+template <int R, int EPT, bool COLM, int DIR, bool PRETW, typename T, int LV, int LM, int LN, int NS, int NT>
+ZM_DEV void stockham_stage_ct(cpx<T> *s, int tid, const tw<T> *twN) {
+    constexpr int NB = EPT / R;
+    constexpr bool CONJ = DIR > 0;
+    constexpr int n = 1 << LN, VEC = 1 << LV, M = 1 << LM, LOGN = LV + LM;
+    constexpr int nR = n / R;
+    constexpr int logR = (R == 2) ? 1 : (R == 4) ? 2 : (R == 8) ? 3 : 4;
+    constexpr int lognR = LN - logR;
+    constexpr int str = COLM ? VEC : 1;
+    cpx<T> v[NB][R];
+    int base[NB], jv[NB];
+#pragma unroll
+    for (int u = 0; u < NB; u++) {
+        const int sig = tid + u * NT;
+        int j, bb, tagn;
+        if constexpr (!COLM) {
+            j = sig & (nR - 1);
+            const int b = sig >> lognR;
+            bb = b << LV;
+            tagn = b & (M - 1);
+        } else {
+            const int k2 = sig & (VEC - 1);
+            const int rest = sig >> LV;
+            j = rest & (nR - 1);
+            const int t = rest >> lognR;
+            bb = (t << LOGN) + k2;
+            tagn = k2;
+        }
+        base[u] = bb;
+        jv[u] = j;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int i = j + r * nR;
+            cpx<T> x = s[bb + i * str];
+            if constexpr (PRETW) x = twmul<CONJ>(x, ldtw(twN, (int64_t)i * tagn));
+            v[u][r] = x;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < NB; u++) {
+        const int j = jv[u];
+        const int k = j & (NS - 1);
+        if constexpr (NS > 1) {
+            constexpr int sh = LOGN - LN + (LN - (ct_log2(NS * R) + 1) + 1);
+#pragma unroll
+            for (int r = 1; r < R; r++) v[u][r] = twmul<CONJ>(v[u][r], ldtw(twN, ((int64_t)k * r) << sh));
+        }
+        dft<R, DIR, T>(v[u]);
+        const int idxD = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) s[base[u] + (idxD + r * NS) * str] = v[u][r];
+    }
+    __syncthreads();
+}
+
+template <int LN, int RL> struct radix_sched {
+    static constexpr int rem = LN % RL;
+    static constexpr int nst = (rem ? 1 : 0) + LN / RL;
+    static constexpr int rad(int i) { return (rem && i == 0) ? (1 << rem) : (1 << RL); }
+};
+
+template <int ST, int NS, int EPT, bool COLM, int DIR, bool PRE, typename T, int LV, int LM, int LN, int NT, int RL>
+ZM_DEV void run_subfft_ct(cpx<T> *s, int tid, const tw<T> *twN) {
+    using SC = radix_sched<LN, RL>;
+    if constexpr (ST < SC::nst) {
+        constexpr int R = SC::rad(ST);
+        stockham_stage_ct<R, EPT, COLM, DIR, PRE && ST == 0, T, LV, LM, LN, NS, NT>(s, tid, twN);
+        run_subfft_ct<ST + 1, NS * R, EPT, COLM, DIR, PRE, T, LV, LM, LN, NT, RL>(s, tid, twN);
+    }
+}
+
+template <typename T, int EPT, bool INV, int LV, int LM, int NT>
+ZM_DEV void tile_transform_ct(cpx<T> *s, int tid, const tw<T> *twN) {
+    constexpr int RL = EPT >= 16 ? 4 : 3;   // radix_schedule(n, EPT): largest radix EPT
+    if constexpr (!INV) {
+        run_subfft_ct<0, 1, EPT, false, -1, false, T, LV, LM, LV, NT, RL>(s, tid, twN);
+        run_subfft_ct<0, 1, EPT, true, -1, true, T, LV, LM, LM, NT, RL>(s, tid, twN);
+    } else {
+        run_subfft_ct<0, 1, EPT, true, 1, false, T, LV, LM, LM, NT, RL>(s, tid, twN);
+        run_subfft_ct<0, 1, EPT, false, 1, true, T, LV, LM, LV, NT, RL>(s, tid, twN);
+    }
+}
+
 // ------------------------------------------------------------ tile addressing
 struct Tile {
     int TL, logT;
