@@ -233,17 +233,18 @@ __global__ void __launch_bounds__(256) stencil_kernel(const S *__restrict__ in, 
     *reinterpret_cast<uint4 *>(out + e * NC) = *reinterpret_cast<const uint4 *>(&res);
 }
 
-// The three 2D stencils in one launch, RY consecutive local rows of one B-row block per
-// thread (the same packed position): the 16-byte vectors of rows lr0 - 2 .. lr0 + RY + 1
-// are loaded once and shared by the RY outputs (RY + 4 row loads instead of 5 RY), and
-// the index arithmetic is done once per thread.  Rows outside the block (above a block's
-// first row group, below its last) go through the block-cyclic maps as in
-// stencil_kernel; every output is computed by the same expressions, in the same order.
-template <typename S, int NC, int RY>
-__global__ void __launch_bounds__(256) stencil_all_rows_kernel(const S *__restrict__ in, S *__restrict__ out,
-                                                               S *__restrict__ out2, S *__restrict__ out3,
-                                                               const Geom g, int64_t nthreads, S coef, S coef2,
-                                                               S rden) {
+// 2D stencils (OP as in stencil_kernel), RY consecutive local rows of one B-row block per
+// thread (the same packed position): the 16-byte vectors of the rows the stencil needs
+// (lr0 - 2 .. lr0 + RY + 1 for dy and the three in one launch, lr0 - 1 .. lr0 + RY for the
+// Laplacian, none beyond the centre rows for dx) are loaded once and shared by the RY
+// outputs, and the index arithmetic is done once per thread.  Rows outside the block
+// (above a block's first row group, below its last) go through the block-cyclic maps as
+// in stencil_kernel; every output is computed by the same expressions, in the same order.
+template <typename S, int NC, int OP, int RY>
+__global__ void __launch_bounds__(256) stencil_rows_kernel(const S *__restrict__ in, S *__restrict__ out,
+                                                           S *__restrict__ out2, S *__restrict__ out3,
+                                                           const Geom g, int64_t nthreads, S coef, S coef2,
+                                                           S rden) {
     using O = ops<S>;
     using V = vec16<S>;
     constexpr int K = V::n / NC;                 // elements per vector
@@ -300,9 +301,52 @@ __global__ void __launch_bounds__(256) stencil_all_rows_kernel(const S *__restri
         }
         return r;
     };
-    V ys[RY + 4];
+    // rows lr0 + d for d in [-H, RY + H), H = the stencil's reach along y
+    constexpr int H = OP == ST_LAPLACE ? 1 : (OP == ST_DX ? 0 : 2);
+    V ys[RY + 2 * H];
 #pragma unroll
-    for (int d = -2; d < RY + 2; d++) ys[d + 2] = rowv(d);
+    for (int d = -H; d < RY + H; d++) ys[d + H] = rowv(d);
+    if constexpr (OP != ST_ALL) {
+        const S den = O::mul((S)12, coef);    // dx / dy: coef = delta
+#pragma unroll
+        for (int r = 0; r < RY; r++) {
+            const int64_t e = e0 + (int64_t)r * L;
+            V res;
+            if constexpr (OP == ST_LAPLACE) {
+                // laplace.cu:91-168 accumulation order
+                const V lf = colv(e, lr0 + r, -1), rt = colv(e, lr0 + r, 1);
+                const V &up = ys[r], &dn = ys[r + 2], &c = ys[r + 1];
+#pragma unroll
+                for (int i = 0; i < V::n; i++) {
+                    S s = O::add((S)0, up.v[i]);
+                    s = O::add(s, dn.v[i]);
+                    s = O::add(s, lf.v[i]);
+                    s = O::add(s, rt.v[i]);
+                    s = O::fmaop((S)(-4), c.v[i], s);
+                    res.v[i] = O::mul(s, coef);
+                }
+            } else {
+                // dx.cu:26-79 / dy.cu:34-100: ((-8 f[-1] + f[-2]) + 8 f[+1]) - f[+2], / (12 delta)
+                V m1, m2, p1, p2;
+                if constexpr (OP == ST_DX) {
+                    m1 = colv(e, lr0 + r, -1); m2 = colv(e, lr0 + r, -2);
+                    p1 = colv(e, lr0 + r, 1); p2 = colv(e, lr0 + r, 2);
+                } else {
+                    m1 = ys[r + 1]; m2 = ys[r]; p1 = ys[r + 3]; p2 = ys[r + 4];
+                }
+#pragma unroll
+                for (int i = 0; i < V::n; i++) {
+                    S s = O::add((S)0, O::mul(m1.v[i], (S)-8));
+                    s = O::add(s, m2.v[i]);
+                    s = O::add(s, O::mul(p1.v[i], (S)8));
+                    s = O::sub(s, p2.v[i]);
+                    res.v[i] = div_den(s, den, rden);
+                }
+            }
+            *reinterpret_cast<uint4 *>(out + e * NC) = *reinterpret_cast<const uint4 *>(&res);
+        }
+        return;
+    }
     const S den = O::mul((S)12, coef2);
 #pragma unroll
     for (int r = 0; r < RY; r++) {
@@ -351,19 +395,27 @@ static cudaError_t launch_s(const zm_plan_s *p, int op, const void *in, void *ou
     const double dl = op == ST_ALL ? coef2 : coef;
     const S rd = (S)(1.0 / (12.0 * dl));
     if (p->g.dim == 2) {
-        if (op == ST_LAPLACE)
+        if (sizeof(S) == 4 && p->g.b % 4 == 0) {
+            // four rows of a B-row block per thread (FP32; the FP64 form stays one row
+            // per thread: its four-row form was slower, 4.20 -> 4.34 ms at N = 16384 for
+            // the three stencils in one launch)
+            const int64_t nt = nvec / 4;
+            const unsigned g4 = (unsigned)((nt + threads - 1) / threads);
+            if (op == ST_LAPLACE)
+                stencil_rows_kernel<S, NC, ST_LAPLACE, 4><<<g4, threads, 0, st>>>(i, o, o2, o3, p->g, nt, c, c2, rd);
+            else if (op == ST_DX)
+                stencil_rows_kernel<S, NC, ST_DX, 4><<<g4, threads, 0, st>>>(i, o, o2, o3, p->g, nt, c, c2, rd);
+            else if (op == ST_DY)
+                stencil_rows_kernel<S, NC, ST_DY, 4><<<g4, threads, 0, st>>>(i, o, o2, o3, p->g, nt, c, c2, rd);
+            else
+                stencil_rows_kernel<S, NC, ST_ALL, 4><<<g4, threads, 0, st>>>(i, o, o2, o3, p->g, nt, c, c2, rd);
+        } else if (op == ST_LAPLACE)
             stencil_kernel<S, NC, ST_LAPLACE, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
         else if (op == ST_DX)
             stencil_kernel<S, NC, ST_DX, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
         else if (op == ST_DY)
             stencil_kernel<S, NC, ST_DY, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
-        else if (sizeof(S) == 4 && p->g.b % 4 == 0) {
-            // four rows of a B-row block per thread (FP32; the FP64 form stays one row
-            // per thread: its four-row form was slower, 4.20 -> 4.34 ms at N = 16384)
-            const int64_t nt = nvec / 4;
-            stencil_all_rows_kernel<S, NC, 4>
-                <<<(unsigned)((nt + threads - 1) / threads), threads, 0, st>>>(i, o, o2, o3, p->g, nt, c, c2, rd);
-        } else
+        else
             stencil_kernel<S, NC, ST_ALL, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
     } else {
         if (op != ST_LAPLACE) return cudaErrorInvalidValue;
