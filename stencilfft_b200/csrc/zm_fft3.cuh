@@ -154,6 +154,9 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
         return a.f_base + (int64_t)(k2 >> g.logVP) * a.f_chunk + (pos0 >> flg) * a.f_hi + (pos0 & ((1 << flg) - 1));
     };
     const int64_t fstep = ((((int64_t)512 >> LV) * VP) >> flg) * a0.f_hi;
+    // contiguous frequency side (inverse input): the elements of threads t, t + 1 (t even,
+    // k2 even, so the same run of VP) are adjacent and 16-byte aligned
+    const bool fpair = INV && PERS && a0.f_hi == 1 && flg == 0 && VP >= 2;
     const bool scl = prm.apply_scale != 0;
     const float sre = (float)prm.scale_re, sim = (float)prm.scale_im;
     auto scale_c = [&](C o) -> C { return scl ? C{o.x * sre - o.y * sim, o.x * sim + o.y * sre} : o; };
@@ -195,8 +198,20 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
             }
         } else {
             const C *ip = in + fofs(b);
+            if (fpair) {
+                // threads t, t + 1 (t even) need adjacent elements: the even one copies
+                // both for kc < 16, the odd one for kc >= 16 (16-byte copies)
+                const int half = tid & 1;
+                const C *ipp = ip - half;
 #pragma unroll
-            for (int kc = 0; kc < 32; kc++) cp_async8(S + kc * 512 + tid, ip + fstep * kc);
+                for (int q = 0; q < 16; q++) {
+                    const int kc = 16 * half + q;
+                    cp_async16(S + kc * 512 + (tid - half), ipp + fstep * kc);
+                }
+            } else {
+#pragma unroll
+                for (int kc = 0; kc < 32; kc++) cp_async8(S + kc * 512 + tid, ip + fstep * kc);
+            }
         }
         cp_async_commit();
     };
@@ -330,6 +345,7 @@ __global__ void __launch_bounds__(512, 1) k3_pass_kernel(const LineParams prm) {
             C y[32];
             if constexpr (PERS) {
                 cp_async_wait_all();
+                if (fpair) __syncwarp();   // the pair partner copied half of this thread's points
 #pragma unroll
                 for (int kc = 0; kc < 32; kc++) y[kc] = S[kc * 512 + tid];
             } else {
