@@ -380,6 +380,95 @@ __global__ void __launch_bounds__(256) stencil_rows_kernel(const S *__restrict__
     }
 }
 
+// 3D Laplacian (laplace3d.cu:98-224 accumulation order) with RX vectors of one line per
+// thread.  A warp takes 32 * RX consecutive 16-byte vectors of one (rank, depth, row) line
+// (lane t: vectors t, t + 32, ..., so every load instruction of the warp stays one
+// contiguous 512-byte run), and the four neighbour lines along y and z (block-cyclic
+// maps with the periodic wrap) are located once per thread for its RX vectors instead of
+// once per vector: the integer index work, not DRAM, bounds the one-vector kernel
+// (stencil_kernel<..., 3>).  Each output is computed by the same expressions in the same
+// order as there.
+template <typename S, int NC, int RX>
+__global__ void __launch_bounds__(256) stencil3d_lines_kernel(const S *__restrict__ in, S *__restrict__ out,
+                                                              const Geom g, int64_t nseg, S coef) {
+    using O = ops<S>;
+    using V = vec16<S>;
+    constexpr int K = V::n / NC;                 // elements per vector
+    const int64_t seg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (seg >= nseg) return;
+    const int lane = (int)(threadIdx.x & 31);
+    const int L = (int)g.L, N = (int)g.n, P = (int)g.p;
+    const int segs_line = L / (K * 32 * RX);     // warps per line
+    const int64_t line = seg / segs_line;        // (rank * L + ld) * L + lr
+    const int v0 = (int)(seg - line * segs_line) * 32 * RX + lane;
+    const int lr = (int)line & (L - 1), ld = (int)(line >> g.logL) & (L - 1);
+    const int rank = (int)(line >> (2 * g.logL));
+    const int cid = rank & (P - 1), rid = (rank >> g.logP) & (P - 1), did = rank >> (2 * g.logP);
+    const int gr = l2g(lr, rid, g), gd = l2g(ld, did, g);
+    // first element of the neighbour lines
+    auto yline = [&](int d) {
+        int id, li;
+        g2l((gr + d + N) & (N - 1), g, id, li);
+        const int rk = (did * P + id) * P + cid;
+        return (((((int64_t)rk << g.logL) + ld) << g.logL) + li) << g.logL;
+    };
+    auto zline = [&](int d) {
+        int id, li;
+        g2l((gd + d + N) & (N - 1), g, id, li);
+        const int rk = (id * P + rid) * P + cid;
+        return (((((int64_t)rk << g.logL) + li) << g.logL) + lr) << g.logL;
+    };
+    const int64_t ec = line << g.logL, eu = yline(-1), ed = yline(1), ef = zline(-1), eb = zline(1);
+    auto ld16 = [&](int64_t el) {
+        V r;
+        *reinterpret_cast<uint4 *>(&r) = __ldg(reinterpret_cast<const uint4 *>(in + el * NC));
+        return r;
+    };
+    // neighbour along x (d = -1 / +1) of the vector at packed position pos (VEC a multiple
+    // of K, checked by the host).  Inside a B-column block it is the vector VEC positions
+    // away.  Across the block edge it is column B - 1 / 0 of the rank to the left / right
+    // at the same cycle jj, except past the end of a block cycle (cid = 0 / P - 1): there
+    // the rank is P - 1 ranks away and the cycle moves by one, so the K neighbours are
+    // shifted by one element (utils.h:122-128) and read one by one.
+    const int64_t l3 = (int64_t)1 << (3 * g.logL);
+    auto colv = [&](int pos, int d) {
+        const int j = pos >> g.logVEC;
+        if (d < 0 ? j > 0 : j < (int)g.b - 1) return ld16(ec + pos + (int64_t)d * (int64_t)g.vec);
+        const bool wrap = d < 0 ? cid == 0 : cid == P - 1;
+        const int64_t e1 = ec + (wrap ? (int64_t)(-d * (P - 1)) : (int64_t)d) * l3 +
+                           (d < 0 ? ((int)g.b - 1) << g.logVEC : 0);
+        const int jj = pos & ((int)g.vec - 1);
+        if (!wrap) return ld16(e1 + jj);
+        V r;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const int64_t ak = e1 + ((jj + k + d) & ((int)g.vec - 1));
+#pragma unroll
+            for (int q = 0; q < NC; q++) r.v[k * NC + q] = __ldg(in + ak * NC + q);
+        }
+        return r;
+    };
+#pragma unroll
+    for (int x = 0; x < RX; x++) {
+        const int pos = (v0 + 32 * x) * K;
+        const V up = ld16(eu + pos), dn = ld16(ed + pos), lf = colv(pos, -1), rt = colv(pos, 1);
+        const V fr = ld16(ef + pos), bk = ld16(eb + pos), c = ld16(ec + pos);
+        V res;
+#pragma unroll
+        for (int i = 0; i < V::n; i++) {
+            S s = O::add((S)0, up.v[i]);
+            s = O::add(s, dn.v[i]);
+            s = O::add(s, lf.v[i]);
+            s = O::add(s, rt.v[i]);
+            s = O::add(s, fr.v[i]);
+            s = O::add(s, bk.v[i]);
+            s = O::fmaop((S)(-6), c.v[i], s);
+            res.v[i] = O::mul(s, coef);
+        }
+        *reinterpret_cast<uint4 *>(out + (ec + pos) * NC) = *reinterpret_cast<const uint4 *>(&res);
+    }
+}
+
 template <typename S, int NC>
 static cudaError_t launch_s(const zm_plan_s *p, int op, const void *in, void *out, void *out2, void *out3,
                             double coef, double coef2, cudaStream_t st) {
@@ -419,7 +508,16 @@ static cudaError_t launch_s(const zm_plan_s *p, int op, const void *in, void *ou
             stencil_kernel<S, NC, ST_ALL, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
     } else {
         if (op != ST_LAPLACE) return cudaErrorInvalidValue;
-        stencil_kernel<S, NC, ST_LAPLACE, 3><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
+        // vectors of one line per thread: 4 for one complex128 per vector, else 2
+        constexpr int RX = K == 1 ? 4 : 2;
+        const int64_t vline = p->g.L / K;       // vectors per line
+        if (vline % (32 * RX) == 0 && p->g.vec % K == 0) {
+            const int64_t nseg = nvec / (32 * RX);
+            const unsigned gs = (unsigned)((nseg * 32 + threads - 1) / threads);
+            stencil3d_lines_kernel<S, NC, RX><<<gs, threads, 0, st>>>(i, o, p->g, nseg, c);
+        } else {
+            stencil_kernel<S, NC, ST_LAPLACE, 3><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
+        }
     }
     count_launch();
     return cudaGetLastError();

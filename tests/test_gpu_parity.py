@@ -124,6 +124,23 @@ def test_laplace_matches_oracle(dim, n, b, p, dt):
 
 
 @pytest.mark.parametrize("dt", ["c128", "c64"])
+@pytest.mark.parametrize("n,b,p", [(128, 8, 2), (256, 16, 2), (256, 4, 4), (256, 64, 2)])
+def test_laplace3d_long_lines_match_oracle(n, b, p, dt):
+    """Lines of 64 (complex64) / 128 (complex128) vectors take the several-vectors-per-
+    thread 3D kernel: every block-boundary and wrap case of x, y and z at a local side of
+    128 (N = 256, P = 2); the side-64 cases keep the one-vector kernel."""
+    import torch
+    x = rand_field(3, n, seed=11)
+    buf = O.natural_to_real_layout(x, b, p)
+    ref = O.laplace(buf, 3, n, b, p)
+    pl = _plan(3, n, b, p, dt)
+    d0 = to_dev(buf, dt)
+    d1 = torch.empty_like(d0)
+    pl.laplace(d0, d1, inv_h2=float(n * n))
+    assert relerr(to_host(d1), ref * n * n) < TOL[dt]
+
+
+@pytest.mark.parametrize("dt", ["c128", "c64"])
 @pytest.mark.parametrize("dim,n,b,p", [c for c in CFG_2D if c[2] >= 2])
 def test_dx_dy_match_oracle(dim, n, b, p, dt):
     import torch
