@@ -162,7 +162,7 @@ ZM_DEV void batch_tile_transform(cpx<T> *s, const BatchField &f, int nthr, int t
 }
 
 template <typename T, int EPT>
-__global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(const BatchParams bp) {
+__global__ void __launch_bounds__(kBatchThreads, 4) batch_kernel(const BatchParams bp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T> *s = reinterpret_cast<cpx<T> *>(smem_raw);
     __shared__ int64_t s_abase[64], s_fbase[64];
@@ -233,19 +233,19 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(const BatchPara
             cpx<T> *out = reinterpret_cast<cpx<T> *>(S.out) + sf.off;
             const tw<T> *twN = reinterpret_cast<const tw<T> *>(sf.twN);
             if (S.op == BOP_X_FWD || S.op == BOP_Y_FWD) {
-                tile_load_vec(c, g, s, in, nthr, tid);
+                tile_load_vec<EPT>(c, g, s, in, nthr, tid);
                 __syncthreads();
                 batch_tile_transform<T, EPT, false>(s, sf, nthr, tid, twN);
-                tile_store_freq(c, g, s, out, false, (T)1, (T)0, nthr, tid);
+                tile_store_freq<EPT>(c, g, s, out, false, (T)1, (T)0, nthr, tid);
             } else if (S.op == BOP_X_INV || S.op == BOP_Y_INV) {
-                tile_load_freq(c, g, s, in, nthr, tid);
+                tile_load_freq<EPT>(c, g, s, in, nthr, tid);
                 __syncthreads();
                 batch_tile_transform<T, EPT, true>(s, sf, nthr, tid, twN);
                 const bool scl = S.scale && xpass;
                 const T sc = (T)(1.0 / ((double)g.n * (double)g.n));
-                tile_store_vec(c, g, s, out, scl, sc, (T)0, nthr, tid);
+                tile_store_vec<EPT>(c, g, s, out, scl, sc, (T)0, nthr, tid);
             } else {   // BOP_Y_POISSON
-                tile_load_vec(c, g, s, in, nthr, tid);
+                tile_load_vec<EPT>(c, g, s, in, nthr, tid);
                 __syncthreads();
                 batch_tile_transform<T, EPT, false>(s, sf, nthr, tid, twN);
                 // slot (t, k1, k2) holds the frequency the y pass would store at rank
@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(kBatchThreads, 3) batch_kernel(const BatchPara
                 }
                 __syncthreads();
                 batch_tile_transform<T, EPT, true>(s, sf, nthr, tid, twN);
-                tile_store_vec(c, g, s, out, false, (T)1, (T)0, nthr, tid);
+                tile_store_vec<EPT>(c, g, s, out, false, (T)1, (T)0, nthr, tid);
             }
         }
     }

@@ -39,15 +39,15 @@ __global__ void __launch_bounds__(1024) line_fft_kernel(const LineParams prm) {
     const tw<T> *twN = reinterpret_cast<const tw<T> *>(prm.twN);
     const Tile c = tile_begin(g, prm.kind, (int64_t)blockIdx.x * prm.T, prm.T, s_abase, s_fbase, nthr, tid);
     __syncthreads();
-    if (!INV) tile_load_vec(c, g, s, in, nthr, tid);
-    else tile_load_freq(c, g, s, in, nthr, tid);
+    if (!INV) tile_load_vec<EPT>(c, g, s, in, nthr, tid);
+    else tile_load_freq<EPT>(c, g, s, in, nthr, tid);
     __syncthreads();
     if (!prm.permute_only)
         tile_transform<T, EPT, INV>(s, g, prm.rad_vec, prm.nst_vec, prm.rad_m, prm.nst_m, nthr, tid, twN);
     const bool scl = prm.apply_scale && !prm.permute_only;
     const T sr = (T)prm.scale_re, si = (T)prm.scale_im;
-    if (!INV) tile_store_freq(c, g, s, out, scl, sr, si, nthr, tid);
-    else tile_store_vec(c, g, s, out, scl, sr, si, nthr, tid);
+    if (!INV) tile_store_freq<EPT>(c, g, s, out, scl, sr, si, nthr, tid);
+    else tile_store_vec<EPT>(c, g, s, out, scl, sr, si, nthr, tid);
 }
 
 // ------------------------------------------------------------------ launch

@@ -255,47 +255,64 @@ ZM_DEV int tile_freq_slot(const Geom &g, int t, int ch, int pos) {
     return (t << g.logN) + (k1 << g.logVEC) + (ch << g.logVP) + f;
 }
 
+// The four sweeps below run exactly EPT elements per thread (e = tid + i * nthr, from
+// nthr * EPT == TL * N).  The loads go to registers first, all EPT of them in flight
+// before any is written to shared memory: one load at a time per thread leaves far too
+// few bytes in flight to cover the DRAM latency.
+
 // vector side -> rows s[t][c*L + pos] = s[t][n1*VEC + n2]
-template <typename T>
+template <int EPT, typename T>
 ZM_DEV void tile_load_vec(const Tile &c, const Geom &g, cpx<T> *s, const cpx<T> *in, int nthr, int tid) {
-    const int tot = c.TL << g.logN;
-    for (int e = tid; e < tot; e += nthr) {
+    cpx<T> v[EPT];
+#pragma unroll
+    for (int i = 0; i < EPT; i++) {
+        const int e = tid + i * nthr;
         const int t = e >> g.logN;
         const int r = e & (int)(g.n - 1);
         const int ch = r >> g.logL, pos = r & (int)(g.L - 1);
-        s[e] = ldg(in + c.abase[t] + ch * c.a_chunk + pos);
+        v[i] = ldg(in + c.abase[t] + ch * c.a_chunk + pos);
     }
+#pragma unroll
+    for (int i = 0; i < EPT; i++) s[tid + i * nthr] = v[i];
 }
 
 // frequency side (t, c, pos = k1*VP + f) -> s[t][k1*VEC + c*VP + f]
-template <typename T>
+template <int EPT, typename T>
 ZM_DEV void tile_load_freq(const Tile &c, const Geom &g, cpx<T> *s, const cpx<T> *in, int nthr, int tid) {
-    const int tot = c.TL << g.logN;
-    for (int e = tid; e < tot; e += nthr) {
+    cpx<T> v[EPT];
+#pragma unroll
+    for (int i = 0; i < EPT; i++) {
         int t, ch, pos;
-        tile_freq_coords(c, g, e, t, ch, pos);
-        s[tile_freq_slot(g, t, ch, pos)] = ldg(in + c.fbase[t] + ch * c.f_chunk + pos * c.f_pos);
+        tile_freq_coords(c, g, tid + i * nthr, t, ch, pos);
+        v[i] = ldg(in + c.fbase[t] + ch * c.f_chunk + pos * c.f_pos);
+    }
+#pragma unroll
+    for (int i = 0; i < EPT; i++) {
+        int t, ch, pos;
+        tile_freq_coords(c, g, tid + i * nthr, t, ch, pos);
+        s[tile_freq_slot(g, t, ch, pos)] = v[i];
     }
 }
 
-template <typename T>
+template <int EPT, typename T>
 ZM_DEV void tile_store_freq(const Tile &c, const Geom &g, const cpx<T> *s, cpx<T> *out, bool scl, T sr,
                             T si, int nthr, int tid) {
-    const int tot = c.TL << g.logN;
-    for (int e = tid; e < tot; e += nthr) {
+#pragma unroll
+    for (int i = 0; i < EPT; i++) {
         int t, ch, pos;
-        tile_freq_coords(c, g, e, t, ch, pos);
+        tile_freq_coords(c, g, tid + i * nthr, t, ch, pos);
         cpx<T> v = s[tile_freq_slot(g, t, ch, pos)];
         if (scl) v = {v.x * sr - v.y * si, v.x * si + v.y * sr};
         out[c.fbase[t] + ch * c.f_chunk + pos * c.f_pos] = v;
     }
 }
 
-template <typename T>
+template <int EPT, typename T>
 ZM_DEV void tile_store_vec(const Tile &c, const Geom &g, const cpx<T> *s, cpx<T> *out, bool scl, T sr,
                            T si, int nthr, int tid) {
-    const int tot = c.TL << g.logN;
-    for (int e = tid; e < tot; e += nthr) {
+#pragma unroll
+    for (int i = 0; i < EPT; i++) {
+        const int e = tid + i * nthr;
         const int t = e >> g.logN;
         const int r = e & (int)(g.n - 1);
         const int ch = r >> g.logL, pos = r & (int)(g.L - 1);
