@@ -421,10 +421,23 @@ def run_ours(args, rank: int, world: int):
 
 
 def run_profile_case(args):
-    """Small profiling case (N = 8192, c64 by default, 512 MiB per buffer): one warm-up
-    and one measured call of each stage, for `ncu -k ... -s/-c` captures."""
+    """Small profiling case (N = 8192, c64 by default, 512 MiB per buffer; or the 3D
+    Laplacian at N = 512): one warm-up and one measured call of each stage, for
+    `ncu -k ... -s/-c` captures."""
     import torch
-    from stencilfft_b200 import Plan
+    from stencilfft_b200 import Plan, abi
+    if args.profile_ops == "lap3d":
+        # 3D 7-point Laplacian, N = 512, P = 4, B = 32 (1 GiB per c64 field, two fields)
+        n3 = 512
+        pl3 = Plan(3, n3, 32, P, dtype=args.profile_dtype)
+        u3, o3 = pl3.empty(), pl3.empty()
+        pl3.fill(u3, abi.ZM_FIELD_GAUSSIAN, 2)
+        for _ in range(2):
+            pl3.laplace(u3, o3, inv_h2=float(n3 * n3))
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": {"dim": 3, "n": n3, "p": P, "b": 32, "dtype": args.profile_dtype,
+                                           "ops": "lap3d", "field_bytes": pl3.field_bytes}}))
+        return
     n = args.profile_n
     pl = Plan(2, n, B, P, dtype=args.profile_dtype)
     modes, amps = modes_and_amps(n)
@@ -470,7 +483,7 @@ def main():
                     help="run the small profiling case only (for ncu captures)")
     ap.add_argument("--profile-n", type=int, default=8192)
     ap.add_argument("--profile-dtype", default="c64")
-    ap.add_argument("--profile-ops", choices=["all", "fwd", "inv"], default="all")
+    ap.add_argument("--profile-ops", choices=["all", "fwd", "inv", "lap3d"], default="all")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.profile_case:
