@@ -1,0 +1,106 @@
+"""CPU check of the 3D Laplacian kernel's neighbour addressing against the oracle's layout.
+
+``stencil3d_lines_kernel`` (stencilfft_b200/csrc/zm_stencil.cu) finds the y / z
+neighbour lines through the block-cyclic maps and the x neighbours across a block edge
+through a closed form (rank +-1, or -+(P - 1) with a one-element shift past the end of a
+block cycle).  This restates that integer arithmetic in numpy and checks every neighbour
+of every element against the real-layout permutation of the oracle (zoracle.c, the
+reference's utils.h index maps): the element at natural (d, r, c +- 1) etc.  It also
+checks that the warp / lane / vector assignment covers every vector once.  The kernel's
+own outputs are checked against the oracle by the GPU parity tests.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+
+
+def lg(x):
+    return int(x).bit_length() - 1
+
+
+def kernel_neighbours(n, b, p, K):
+    """Element index of each neighbour of each element, as the kernel computes it:
+    returns {name: array over all elements e of the real layout}."""
+    L = n // p
+    vec = L // b
+    logB, logP, logL, logVEC = lg(b), lg(p), lg(L), lg(vec)
+    total = L ** 3 * p ** 3
+    e = np.arange(total, dtype=np.int64)
+    line, pos_e = e >> logL, e & (L - 1)
+    k = pos_e & (K - 1)                  # element inside its 16-byte vector
+    pos = pos_e - k                      # the vector's first packed position
+    lr, ld, rank = line & (L - 1), (line >> logL) & (L - 1), line >> (2 * logL)
+    cid, rid, did = rank & (p - 1), (rank >> logP) & (p - 1), rank >> (2 * logP)
+
+    def l2g(li, i):
+        return ((li >> logB) << (logB + logP)) + (i << logB) + (li & (b - 1))
+
+    def g2l(gi):
+        return (gi >> logB) & (p - 1), ((gi >> (logB + logP)) << logB) + (gi & (b - 1))
+
+    gr, gd = l2g(lr, rid), l2g(ld, did)
+    ec = line << logL
+    out = {}
+    for d, nm in ((-1, "up"), (1, "dn")):
+        i, li = g2l((gr + d + n) & (n - 1))
+        rk = (did * p + i) * p + cid
+        out[nm] = (((((rk << logL) + ld) << logL) + li) << logL) + pos + k
+    for d, nm in ((-1, "fr"), (1, "bk")):
+        i, li = g2l((gd + d + n) & (n - 1))
+        rk = (i * p + rid) * p + cid
+        out[nm] = (((((rk << logL) + li) << logL) + lr) << logL) + pos + k
+    l3 = L ** 3
+    j, jj = pos >> logVEC, pos & (vec - 1)
+    for d, nm in ((-1, "lf"), (1, "rt")):
+        inside = j > 0 if d < 0 else j < b - 1
+        wrap = cid == 0 if d < 0 else cid == p - 1
+        e1 = ec + np.where(wrap, -d * (p - 1), d) * l3 + ((b - 1) << logVEC if d < 0 else 0)
+        edge = np.where(wrap, e1 + ((jj + k + d) & (vec - 1)), e1 + jj + k)
+        out[nm] = np.where(inside, ec + pos + k + d * vec, edge)
+    return out
+
+
+def true_neighbours(n, b, p):
+    fwd = O.real_layout_map(3, n, b, p)          # real element -> natural index
+    inv = O.real_layout_inverse_map(3, n, b, p)  # natural index -> real element
+    d, r, c = fwd // (n * n), (fwd // n) % n, fwd % n
+    nat = lambda dd, rr, cc: ((dd % n) * n + rr % n) * n + cc % n
+    return {"up": inv[nat(d, r - 1, c)], "dn": inv[nat(d, r + 1, c)],
+            "lf": inv[nat(d, r, c - 1)], "rt": inv[nat(d, r, c + 1)],
+            "fr": inv[nat(d - 1, r, c)], "bk": inv[nat(d + 1, r, c)]}
+
+
+# (N, B, P) with P dividing VEC = N / (P B); P = 1, 2, 4, 8 and VEC from 1 to 8
+CONFIGS = [(16, 2, 2), (32, 2, 4), (32, 4, 2), (64, 4, 4), (64, 8, 2), (64, 16, 2),
+           (128, 2, 8), (16, 16, 1), (32, 8, 1)]
+
+
+@pytest.mark.parametrize("n,b,p", CONFIGS)
+@pytest.mark.parametrize("K", [1, 2])
+def test_laplace3d_neighbours_match_layout(n, b, p, K):
+    vec = n // p // b
+    if vec % K:
+        pytest.skip("the kernel needs VEC to be a multiple of the elements per vector")
+    got, ref = kernel_neighbours(n, b, p, K), true_neighbours(n, b, p)
+    for nm in ref:
+        assert np.array_equal(got[nm], ref[nm]), nm
+
+
+@pytest.mark.parametrize("L,K,RX", [(64, 1, 2), (128, 1, 4), (128, 2, 2), (256, 2, 2)])
+def test_laplace3d_warp_assignment_covers_each_vector_once(L, K, RX):
+    lines = 64                           # any count: the map is per line
+    nvec = lines * L // K
+    nseg = nvec // (32 * RX)
+    segs_line = L // (K * 32 * RX)
+    tid = np.arange(nseg * 32, dtype=np.int64)
+    seg, lane = tid >> 5, tid & 31
+    line = seg // segs_line
+    v0 = (seg - line * segs_line) * 32 * RX + lane
+    first = np.concatenate([line * L + (v0 + 32 * x) * K for x in range(RX)])
+    assert np.array_equal(np.sort(first), np.arange(0, lines * L, K))
+    # each warp instruction reads 32 consecutive vectors of one line
+    for x in range(RX):
+        pos = (v0 + 32 * x) * K
+        w = pos.reshape(-1, 32)
+        assert (np.diff(w, axis=1) == K).all() and (w[:, -1] < L).all()
