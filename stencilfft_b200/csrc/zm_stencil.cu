@@ -12,12 +12,15 @@
 // in the reference's order (above, below, left, right[, front, back], then the
 // centre term), so the 2D Laplacian and dx / dy are bit-identical to it in FP64.
 //
-// Each thread handles one 16-byte vector of the field (two complex64, one
-// complex128, four float or two double values).  The elements of a vector share a
-// row and a packed vector j, so every neighbour along y or z is again one aligned
-// 16-byte vector; along x it is one too except where the step crosses into the
-// left / right rank at the periodic wrap (utils.h:122-128: the shift by one
-// element at cid = 0 / P-1), which is read element by element.
+// The unit of work is one 16-byte vector of the field (two complex64, one
+// complex128, four float or two double values): one per thread in stencil_kernel,
+// four rows of a B-row block per thread in stencil_rows_kernel (2D, FP32) and two or
+// four vectors of one line per thread in stencil3d_lines_kernel (3D Laplacian, long
+// lines).  The elements of a vector share a row and a packed vector j, so every
+// neighbour along y or z is again one aligned 16-byte vector; along x it is one too
+// except where the step crosses into the left / right rank at the periodic wrap
+// (utils.h:122-128: the shift by one element at cid = 0 / P-1), which is read element
+// by element.
 #include "zm_common.cuh"
 #include "zm_internal.h"
 
