@@ -14,8 +14,9 @@ complex128 form is measured beside it.
 Prints one JSON line (rank 0).  `value` is the device time of one step (ms, max over
 ranks, lower is better).  With --gpus N > 1 (torchrun) every rank runs an independent
 replica (the path is held on one GPU; there is no data-path collective).
-The reference arm (--impl reference) times the CPU restatement of the reference's
-pipeline (oracle/, FP64, all host threads) on a bounded sample of the same workload.
+The reference arm (--impl reference) times the same step on the host cores at the full
+size in complex128: pocketfft (scipy.fft, the stand-in for the reference's FFTW baseline)
+for the transforms and the oracle's OpenMP restatement of the reference's stencils.
 """
 from __future__ import annotations
 
@@ -37,8 +38,6 @@ NMODES, NOISE, MODE_SEED, NOISE_SEED = 32, 1e-3, 1, 1
 METRIC = "fft_stencil_step_time"
 WORKLOAD = ("2D N=16384 P=4 B=64: forward FFT + inverse FFT + 5-pt Laplacian + dx + dy "
             "(h=1/N, the three stencils in one launch) on 32 seeded Fourier modes + 1e-3 noise")
-# CPU sample: the same pipeline on an N=4096 grid (P=4, B=64), scaled to N=16384 by work
-CPU_SAMPLE_N = 4096
 
 
 def modes_and_amps(n: int):
@@ -172,52 +171,95 @@ def max_over_ranks(value: float, dist=None, device: str = "cuda") -> float:
 
 # ------------------------------------------------------------------ CPU arm
 
-def cpu_sample(threads: int | None = None):
-    """Time the oracle (C restatement of the reference pipeline, FP64, OpenMP) on the
-    N=4096 sample and scale each part to N=16384 by its work."""
-    import numpy as np
-    import oracle as O
-    if threads:
-        O.set_threads(threads)
-    cores = O.max_threads()
-    n = CPU_SAMPLE_N
-    dim = 2
-    x = (O.uniform_field(0, n * n)).reshape(n, n)
-    buf = O.natural_to_real_layout(x, B, P)
-    t0 = time.perf_counter()
-    spec = O.forward_fft(buf, dim, n, B, P)
-    back = O.inverse_fft(spec, dim, n, B, P, scale=1.0 / n ** 2)
-    t1 = time.perf_counter()
-    O.laplace(back, dim, n, B, P)
-    O.dx(back, n, B, P, 1.0 / n)
-    O.dy(back, n, B, P, 1.0 / n)
-    t2 = time.perf_counter()
-    fft_scale = (N * N * math.log2(N * N)) / (n * n * math.log2(n * n))
-    st_scale = (N * N) / (n * n)
-    ms = ((t1 - t0) * fft_scale + (t2 - t1) * st_scale) * 1e3
-    sample = (f"oracle (C restatement of the reference pipeline, FP64, OpenMP) on N={n} P={P} B={B}: "
-              f"fwd+inv {1e3 * (t1 - t0):.1f} ms x{fft_scale:.2f} (N^2 log N), "
-              f"lap+dx+dy {1e3 * (t2 - t1):.1f} ms x{st_scale:.0f} (N^2)")
-    return ms, cores, sample
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+class CpuStep:
+    """The step on the host cores at the full size, N = 16384, complex128 (the
+    reference's only precision; FP64 throughout).
+
+    The reference's CPU baseline is FFTW through heFFTe (heffte/heffte_example_fftw.cpp),
+    which is not installed; its stand-in is pocketfft (`scipy.fft.fft2` / `ifft2`, all
+    host threads) on the natural-layout field.  The stencils are the oracle's OpenMP C
+    restatement of the reference's laplace / dx / dy kernels with their halo exchanges
+    (zmodel/stencils/laplace.cu:73-256, dx.cu:10-161, dy.cu:10-185) on the interleaved
+    layout, all host threads.  One step = fft2 + ifft2 + Laplacian + dx + dy."""
+
+    def __init__(self, threads: int | None = None):
+        import numpy as np  # noqa: F401
+        import oracle as O
+        self.threads = threads or cpu_threads()
+        O.set_threads(self.threads)
+        self.x = O.uniform_field(0, N * N).reshape(N, N)
+        self.buf = O.natural_to_real_layout(self.x, B, P)
+
+    def run(self):
+        """(ms of the two transforms, ms of the three stencils)."""
+        import scipy.fft
+        import oracle as O
+        t0 = time.perf_counter()
+        X = scipy.fft.fft2(self.x, workers=self.threads)
+        back = scipy.fft.ifft2(X, workers=self.threads, overwrite_x=True)
+        del X, back
+        t1 = time.perf_counter()
+        for f in (lambda: O.laplace(self.buf, 2, N, B, P), lambda: O.dx(self.buf, N, B, P, 1.0 / N),
+                  lambda: O.dy(self.buf, N, B, P, 1.0 / N)):
+            out = f()
+            del out
+        t2 = time.perf_counter()
+        return (t1 - t0) * 1e3, (t2 - t1) * 1e3
+
+    def describe(self, fft_ms: float, st_ms: float, runs: int) -> str:
+        return (f"full workload N={N} complex128 on {self.threads} threads of {cpu_model()}: "
+                f"pocketfft fft2+ifft2 (scipy.fft, the FFTW stand-in) {fft_ms:.0f} ms + oracle OpenMP "
+                f"laplace+dx+dy on the interleaved layout {st_ms:.0f} ms; median of {runs} steps")
+
+
+def cpu_baseline_sample(runs: int = 3):
+    """The bounded CPU sample of the GPU arm: one warm-up step and the median of `runs`."""
+    step = CpuStep()
+    step.run()
+    res = [step.run() for _ in range(runs)]
+    tot = [a + b for a, b in res]
+    k = tot.index(statistics.median(tot)) if runs % 2 else 0
+    ms = statistics.median(tot)
+    return ms, step.threads, step.describe(res[k][0], res[k][1], runs)
 
 
 def run_reference(args, rank: int, world: int):
+    """The reference arm: every step is the whole workload on the host cores (CpuStep)."""
     if rank != 0:
         return
+    step = CpuStep()
     for _ in range(args.warmup):
-        cpu_sample()
-    times = []
-    cores, sample = None, None
-    for _ in range(args.steps):
-        ms, cores, sample = cpu_sample()
-        times.append(ms)
-    v = statistics.mean(times)
-    line = {"metric": METRIC, "value": v, "unit": "ms", "impl": "reference", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n": N, "p": P, "b": B},
-            "cpu_baseline": {"value": v, "unit": "ms", "cores": cores, "kind": "port", "sample": sample},
-            "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        step.run()
+    res = [step.run() for _ in range(args.steps)]
+    tot = [a + b for a, b in res]
+    v = statistics.mean(tot)
+    med = statistics.median(tot)
+    sample = step.describe(statistics.mean(a for a, _ in res), statistics.mean(b for _, b in res), args.steps)
+    line = {"metric": METRIC, "value": round(v, 2), "unit": "ms", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 2), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (U[-1,1) seed 0)",
+            "config": {"workload": WORKLOAD, "n": N, "p": P, "b": B, "dtype": "c128 (FP64, the reference's only form)"},
+            "median_ms": round(med, 2),
+            "cpu_baseline": {"value": round(v, 2), "unit": "ms", "cores": step.threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(v, 2), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -384,7 +426,7 @@ def run_ours(args, rank: int, world: int):
     stages["laplace_dx_dy"]["note"] = "three stencils in one launch: 6F algorithmic, 4F moved"
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cms, cores, sample = cpu_sample()
+        cms, cores, sample = cpu_baseline_sample()
         cpu = {"value": round(cms, 2), "unit": "ms", "cores": cores, "kind": "port", "sample": sample}
     if rank != 0:
         return

@@ -57,6 +57,12 @@ enum zm_dtype {
                                       (zmodel/transforms/fft.cu:176-180, 211-213) */
 #define ZM_FLAG_HOST_ONLY 0x2u     /* no device resources: the plan answers zm_plan_get_info and
                                       the index maps only (device calls return ZM_ERR_UNSUPPORTED) */
+#define ZM_FLAG_OWN_WORKSPACE 0x4u /* the plan allocates one field of workspace at creation and
+                                      uses it whenever a transform is called with work = NULL:
+                                      the input is then preserved and the 2D transforms take their
+                                      out-of-place configurations.  Calls that pass work = NULL
+                                      share that workspace, so they must not overlap on the GPU
+                                      (two streams at once); pass separate workspaces there. */
 
 typedef struct zm_plan_s *zm_plan;
 
@@ -140,7 +146,8 @@ int zm_autotune_b(int dim, int64_t n, int64_t p, int dtype, int reps, int64_t *b
  *
  * `in` and `out` must not overlap.  `work` may be NULL, in which case `in` is
  * used as scratch and clobbered -- the reference's own contract (input in
- * device_buf0, output in device_buf1, buf0 clobbered; fft.cu:189-198) -- or a
+ * device_buf0, output in device_buf1, buf0 clobbered; fft.cu:189-198) -- unless the
+ * plan was created with ZM_FLAG_OWN_WORKSPACE, whose workspace is then used; or a
  * buffer of zm_plan_workspace_size bytes, in which case `in` is preserved.  The
  * 2D forward transform never touches `in`.  With ZM_FLAG_PERMUTE_ONLY the calls
  * reproduce the reference's do_compute=false pipelines (pure data movement).
@@ -164,7 +171,9 @@ int zm_fft_inverse(zm_plan plan, const void *in, void *out, void *work, double s
  *     fields return ZM_ERR_WORKSPACE.
  *   - The first call on each device looks up the array's device address
  *     (cudaGetSymbolAddress) with that device current; make that first call before
- *     any stream capture.
+ *     any stream capture.  The address is kept for the life of the process:
+ *     cudaDeviceReset on a device makes it stale, so do not call this function on a
+ *     device after resetting it.
  *   - All calls on a device share the one array, which keeps the previous call's
  *     contents.  Each call overwrites everything it later reads, so nothing needs
  *     clearing, but calls that overlap on the GPU (e.g. on two streams at once) race.
@@ -280,7 +289,9 @@ int zm_global_to_reciprocal(zm_plan plan, int64_t kd, int64_t kr, int64_t kc, in
  * call allocates or synchronises, so a sequence of calls can be captured in a CUDA graph.
  * Fields need 64 <= N <= 4096 (complex64) or 32 <= N <= 2048 (complex128).  A grid
  * barrier that waits more than 2 s sets a device error flag instead of hanging:
- * zm_batch_status reads and clears it.
+ * zm_batch_status reads and clears it.  A timeout ends only the launch it happened in
+ * (whose outputs are then incomplete); later calls run normally, and the flag stays set
+ * until zm_batch_status is called, so check it before trusting a call's outputs.
  */
 typedef struct zm_batch_s *zm_batch;
 typedef struct {

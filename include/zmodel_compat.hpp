@@ -44,23 +44,32 @@ struct FftHostPlans {
 
 // FftBuffers (zmodel/transforms/fft.h:9-26): only the device buffers remain; the
 // pinned host staging buffers and the L x L twiddle tables are not needed.  `work`
-// is optional (nullptr reproduces the reference's buf0-is-scratch behaviour).
+// is optional: nullptr uses the plan's own workspace (init_plans default), or buf0 as
+// scratch when the plan has none (the reference's behaviour).
 struct FftBuffers {
     void *device_buf0 = nullptr;
     void *device_buf1 = nullptr;
     void *work = nullptr;
 };
 
+// The compute plan owns one field of workspace by default (ZM_FLAG_OWN_WORKSPACE), so
+// forward_fft / inverse_fft with buffers.work == nullptr run the out-of-place
+// configurations (the fast ones; buf0 is then left intact, which the reference's
+// contract permits).  The reference's init_buffers holds more than that: two to three
+// fields of L x L twiddle tables per rank (fft.cu:75-108).  own_workspace = false keeps
+// device memory to the caller's buffers and uses buf0 as scratch.
 inline void init_plans(FftHostPlans &p, long long n, long long b, long long pdim,
-                       int dtype = ZM_C128) {
+                       int dtype = ZM_C128, bool own_workspace = true) {
     p.dim = 2;
-    ZM_COMPAT_CHECK(zm_plan_create(&p.plan, 2, n, b, pdim, dtype, 0));
+    ZM_COMPAT_CHECK(zm_plan_create(&p.plan, 2, n, b, pdim, dtype,
+                                   own_workspace ? ZM_FLAG_OWN_WORKSPACE : 0u));
     ZM_COMPAT_CHECK(zm_plan_create(&p.permute, 2, n, b, pdim, dtype, ZM_FLAG_PERMUTE_ONLY));
 }
 inline void init_plans_3d(FftHostPlans &p, long long n, long long b, long long pdim,
-                          int dtype = ZM_C128) {
+                          int dtype = ZM_C128, bool own_workspace = true) {
     p.dim = 3;
-    ZM_COMPAT_CHECK(zm_plan_create(&p.plan, 3, n, b, pdim, dtype, 0));
+    ZM_COMPAT_CHECK(zm_plan_create(&p.plan, 3, n, b, pdim, dtype,
+                                   own_workspace ? ZM_FLAG_OWN_WORKSPACE : 0u));
     ZM_COMPAT_CHECK(zm_plan_create(&p.permute, 3, n, b, pdim, dtype, ZM_FLAG_PERMUTE_ONLY));
 }
 #if defined(N_DIM) && defined(B_DIM) && defined(P_DIM)

@@ -23,6 +23,7 @@ ZM_C128 = 0
 ZM_C64 = 1
 ZM_FLAG_PERMUTE_ONLY = 0x1
 ZM_FLAG_HOST_ONLY = 0x2
+ZM_FLAG_OWN_WORKSPACE = 0x4
 
 ZM_SPECTRAL_GAUSSIAN = 0
 ZM_SPECTRAL_POISSON = 1

@@ -223,6 +223,7 @@ static int forward_impl(zm_plan p, const void *in, void *out, void *work, bool s
                         double sim, cudaStream_t st) {
     int rc;
     if ((rc = check_device_plan(p))) return rc;
+    if (!work) work = p->own_work;   // NULL unless ZM_FLAG_OWN_WORKSPACE
     if ((rc = check_field(p, in, "in")) || (rc = check_field(p, out, "out"))) return rc;
     const size_t F = p->total * p->elem_bytes;
     if (overlap(in, out, F)) return fail(ZM_ERR_INVALID_ARG, "in and out overlap");
@@ -255,6 +256,7 @@ static int inverse_impl(zm_plan p, const void *in, void *out, void *work, double
                         cudaStream_t st) {
     int rc;
     if ((rc = check_device_plan(p))) return rc;
+    if (!work) work = p->own_work;   // NULL unless ZM_FLAG_OWN_WORKSPACE
     if ((rc = check_field(p, in, "in")) || (rc = check_field(p, out, "out"))) return rc;
     const size_t F = p->total * p->elem_bytes;
     if (overlap(in, out, F)) return fail(ZM_ERR_INVALID_ARG, "in and out overlap");
@@ -287,8 +289,10 @@ int zm_plan_create(zm_plan *plan, int dim, int64_t n, int64_t b, int64_t p, int 
     *plan = nullptr;
     if (dim != 2 && dim != 3) return fail(ZM_ERR_INVALID_ARG, "dim must be 2 or 3 (got %d)", dim);
     if (dtype != ZM_C128 && dtype != ZM_C64) return fail(ZM_ERR_INVALID_ARG, "unknown dtype %d", dtype);
-    if (flags & ~(ZM_FLAG_PERMUTE_ONLY | ZM_FLAG_HOST_ONLY))
+    if (flags & ~(ZM_FLAG_PERMUTE_ONLY | ZM_FLAG_HOST_ONLY | ZM_FLAG_OWN_WORKSPACE))
         return fail(ZM_ERR_INVALID_ARG, "unknown flags 0x%x", flags);
+    if ((flags & ZM_FLAG_HOST_ONLY) && (flags & ZM_FLAG_OWN_WORKSPACE))
+        return fail(ZM_ERR_INVALID_ARG, "ZM_FLAG_OWN_WORKSPACE needs device resources (not HOST_ONLY)");
     if (!pow2(n) || !pow2(b) || !pow2(p))
         return fail(ZM_ERR_CONSTRAINT, "N=%lld, B=%lld, P=%lld must be powers of two", (long long)n,
                     (long long)b, (long long)p);
@@ -333,6 +337,7 @@ int zm_plan_create(zm_plan *plan, int dim, int64_t n, int64_t b, int64_t p, int 
     // tables w_VEC^m, w_M^m.  All four tables share one allocation of 16-byte entries.
     P->twN = P->twv = P->twm = P->twd = nullptr;
     P->dev_err = nullptr;
+    P->own_work = nullptr;
     if (flags & ZM_FLAG_HOST_ONLY) {
         *plan = P;
         return ZM_OK;
@@ -375,6 +380,15 @@ int zm_plan_create(zm_plan *plan, int dim, int64_t n, int64_t b, int64_t p, int 
     P->twv = tb + (size_t)2 * n * 16;
     P->twm = tb + (size_t)(2 * n + g.vec) * 16;
     P->dev_err = reinterpret_cast<int *>(tb + (size_t)(2 * n + g.vec + g.m) * 16);   // zeroed by the upload
+    if (flags & ZM_FLAG_OWN_WORKSPACE) {
+        e = cudaMalloc(&P->own_work, (size_t)P->total * P->elem_bytes);
+        if (e != cudaSuccess) {
+            P->own_work = nullptr;
+            cudaFree(tables);
+            delete P;
+            return fail(ZM_ERR_NO_MEMORY, "plan workspace allocation failed: %s", cudaGetErrorString(e));
+        }
+    }
     *plan = P;
     return ZM_OK;
 }
@@ -382,6 +396,7 @@ int zm_plan_create(zm_plan *plan, int dim, int64_t n, int64_t b, int64_t p, int 
 int zm_plan_destroy(zm_plan plan) {
     if (!plan) return fail(ZM_ERR_INVALID_ARG, "null plan");
     if (plan->twN) cudaFree(plan->twN);
+    if (plan->own_work) cudaFree(plan->own_work);
     delete plan;
     return ZM_OK;
 }

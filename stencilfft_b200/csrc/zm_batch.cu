@@ -69,7 +69,8 @@ struct BatchParams {
     int nsteps;
     BatchStep step[kMaxSteps];
     unsigned *bar;     // [0] arrivals, [1] generation
-    int *err;          // set to 1 by a barrier that timed out
+    int *abort;        // this launch only: set by a barrier that timed out, the others give up
+    int *err;          // sticky: set by a barrier that timed out, read and cleared by zm_batch_status
     unsigned missing;  // arrivals a barrier waits for beyond the grid (0; > 0 only in the probe)
 };
 
@@ -81,14 +82,16 @@ ZM_DEV unsigned long long globaltimer_ns() {
 
 // Grid-wide barrier of a cooperative launch (all CTAs resident).  Sense by generation
 // count; the last CTA to arrive resets the arrival count and releases the generation.
-// A wait longer than kBarrierTimeoutNs, or a flag already raised by another CTA, makes
-// every waiting CTA give up: returns false and the kernel returns.
-ZM_DEV bool grid_barrier(unsigned *bar, unsigned nblocks, int *err, int *s_ok) {
+// A wait longer than kBarrierTimeoutNs, or an abort already raised by another CTA of
+// this launch, makes every waiting CTA give up: returns false and the kernel returns.
+// A timeout also raises the sticky error word that zm_batch_status reports; the abort
+// word is cleared before every launch, so one timeout ends only its own launch.
+ZM_DEV bool grid_barrier(unsigned *bar, unsigned nblocks, int *abort, int *err, int *s_ok) {
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
         cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(bar[0]), gen(bar[1]);
-        cuda::atomic_ref<int, cuda::thread_scope_device> flag(*err);
+        cuda::atomic_ref<int, cuda::thread_scope_device> flag(*abort), sticky(*err);
         const unsigned g0 = gen.load(cuda::memory_order_acquire);
         if (cnt.fetch_add(1u, cuda::memory_order_acq_rel) == nblocks - 1) {
             cnt.store(0u, cuda::memory_order_relaxed);
@@ -99,6 +102,7 @@ ZM_DEV bool grid_barrier(unsigned *bar, unsigned nblocks, int *err, int *s_ok) {
                 if (flag.load(cuda::memory_order_relaxed) != 0 ||
                     globaltimer_ns() - t0 > kBarrierTimeoutNs) {
                     flag.store(1, cuda::memory_order_relaxed);
+                    sticky.store(1, cuda::memory_order_relaxed);
                     ok = 0;
                     break;
                 }
@@ -171,7 +175,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batch_kernel(const BatchPara
     const int tid = threadIdx.x, nthr = blockDim.x;
 
     for (int st = 0; st < bp.nsteps; st++) {
-        if (st > 0 && !grid_barrier(bp.bar, gridDim.x + bp.missing, bp.err, &s_ok)) return;
+        if (st > 0 && !grid_barrier(bp.bar, gridDim.x + bp.missing, bp.abort, bp.err, &s_ok)) return;
         const BatchStep S = bp.step[st];
         if (S.op == BOP_NOP) continue;
 
@@ -319,7 +323,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batch_kernel(const BatchPara
 template <typename T, int EPT>
 static cudaError_t launch_batch_t(const BatchParams &bp, int grid, cudaStream_t st) {
     const size_t smem = sizeof(cpx<T>) * kBatchThreads * EPT;
-    cudaError_t e = cudaMemsetAsync(bp.bar, 0, 2 * sizeof(unsigned), st);
+    cudaError_t e = cudaMemsetAsync(bp.bar, 0, 3 * sizeof(unsigned), st);   // arrivals, generation, abort
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)grid);
@@ -359,7 +363,7 @@ struct zm_batch_s {
     std::vector<zm::BatchField> fields;    // host copy
     std::vector<int> field_plan;
     zm::BatchField *d_fields = nullptr;
-    unsigned *d_sync = nullptr;            // [0..1] barrier, [2] error flag
+    unsigned *d_sync = nullptr;            // [0..1] barrier, [2] abort (per launch), [3] sticky error flag
     int64_t tiles = 0, elems = 0;
 };
 
@@ -392,7 +396,8 @@ int launch(zm_batch b, const zm::BatchStep *steps, int nsteps, void *stream, uns
     bp.nsteps = nsteps;
     for (int i = 0; i < nsteps; i++) bp.step[i] = steps[i];
     bp.bar = b->d_sync;
-    bp.err = reinterpret_cast<int *>(b->d_sync + 2);
+    bp.abort = reinterpret_cast<int *>(b->d_sync + 2);
+    bp.err = reinterpret_cast<int *>(b->d_sync + 3);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     cudaError_t e = b->dtype == ZM_C128 ? zm::launch_batch_t<double, 8>(bp, b->grid, st)
                                         : zm::launch_batch_t<float, 16>(bp, b->grid, st);
@@ -580,7 +585,7 @@ int zm_batch_status(zm_batch batch, int *device_error) {
     if (e != cudaSuccess)
         return zm::report_error(ZM_ERR_CUDA, "batch status: %s (%s)", cudaGetErrorName(e), cudaGetErrorString(e));
     int flag = 0;
-    e = cudaMemcpy(&flag, batch->d_sync + 2, sizeof(int), cudaMemcpyDeviceToHost);
+    e = cudaMemcpy(&flag, batch->d_sync + 3, sizeof(int), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess && flag) e = cudaMemset(batch->d_sync, 0, 4 * sizeof(unsigned));
     if (e != cudaSuccess)
         return zm::report_error(ZM_ERR_CUDA, "batch status: %s (%s)", cudaGetErrorName(e), cudaGetErrorString(e));

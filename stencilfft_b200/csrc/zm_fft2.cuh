@@ -524,16 +524,26 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
             }
         };
         unsigned parity = 0;
+        // Set (block-uniformly) when a tile's copies did not land within two bounded
+        // waits: the CTA then issues no further copies, so at most that one round can be
+        // in flight when it exits, and it skips the waits of later tiles.  It still runs
+        // its remaining tiles (on stale data, with the device error word raised) so that
+        // the cluster's barriers stay matched.
+        bool copies_lost = false;
         int64_t tile = blockIdx.x / CL;
         if (tile < ntiles) issue(tile);
         for (; tile < ntiles; tile += ncl) {
             __syncthreads();   // the previous tile is done with S and the bases
             set_tile(tile * TL);
-            if (!mbar_wait(&s_bar, parity, kCopyWaitNs)) {
-                if (prm.err) atomicExch(prm.err, 1);
-                mbar_wait(&s_bar, parity, kCopyWaitNs);   // let copies in flight land, bounded
+            if (!copies_lost) {
+                bool landed = mbar_wait(&s_bar, parity, kCopyWaitNs);
+                if (!landed) {
+                    if (prm.err) atomicExch(prm.err, 1);
+                    landed = mbar_wait(&s_bar, parity, kCopyWaitNs);   // let copies in flight land, bounded
+                }
+                copies_lost = __syncthreads_or(!landed) != 0;
+                parity ^= 1u;
             }
-            parity ^= 1u;
             // first row stage: staging -> RA1-point transforms -> rows X
             {
                 constexpr int NU = EPT / RA1;
@@ -554,7 +564,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
                 }
             }
             __syncthreads();   // staging consumed, rows complete, bases visible
-            if (tile + ncl < ntiles) issue(tile + ncl);
+            if (!copies_lost && tile + ncl < ntiles) issue(tile + ncl);
             fwd_row_stage2_scatter();
             tile_sync<CL>();
             fwd_columns();

@@ -67,4 +67,5 @@ struct zm_plan_s {
     int variant;      // tile-shape variant of the size-specialised kernel
     int nvariants;    // variants available for (VEC, M, dtype); 0 = runtime-sized kernel only
     int *dev_err;     // device error word (bounded waits that gave up), inside the tables allocation
+    void *own_work;   // ZM_FLAG_OWN_WORKSPACE: one field, used by transforms called with work = NULL
 };

@@ -42,6 +42,8 @@ extern "C" int zm_fft_inverse_static(zm_plan plan, const void *in, void *out, do
     {
         // First call on this device: the symbol's device address, looked up with this
         // device current.  The host-side name of the array is not a device address.
+        // It is cached for the process's life; a cudaDeviceReset would make it stale
+        // (the header tells callers not to use this function after one).
         std::lock_guard<std::mutex> lock(g_scratch_mu);
         if (!g_scratch_addr[dev]) {
             void *p = nullptr;

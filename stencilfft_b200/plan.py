@@ -40,10 +40,13 @@ class Plan:
     """Immutable description of an N^dim field on a P^dim virtual-rank grid with B x B blocks."""
 
     def __init__(self, dim: int, n: int, b: int, p: int, dtype="c128", permute_only: bool = False,
-                 host_only: bool = False):
-        """host_only: no device resources (ZM_FLAG_HOST_ONLY) -- sizes and index maps only."""
+                 host_only: bool = False, own_workspace: bool = False):
+        """host_only: no device resources (ZM_FLAG_HOST_ONLY) -- sizes and index maps only.
+        own_workspace: the plan holds one field of workspace (ZM_FLAG_OWN_WORKSPACE), used by
+        transforms called without `work`; such calls must not overlap on two streams."""
         self._h = ctypes.c_void_p()
-        flags = (abi.ZM_FLAG_PERMUTE_ONLY if permute_only else 0) | (abi.ZM_FLAG_HOST_ONLY if host_only else 0)
+        flags = ((abi.ZM_FLAG_PERMUTE_ONLY if permute_only else 0) | (abi.ZM_FLAG_HOST_ONLY if host_only else 0)
+                 | (abi.ZM_FLAG_OWN_WORKSPACE if own_workspace else 0))
         if dtype not in _DT:
             raise ValueError(f"dtype must be 'c128' or 'c64', got {dtype!r}")
         check(lib().zm_plan_create(ctypes.byref(self._h), int(dim), int(n), int(b), int(p),

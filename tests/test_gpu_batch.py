@@ -172,3 +172,20 @@ def test_barrier_timeout_is_reported_not_hung():
     for i, (n, b, p) in enumerate(MIXED[:3]):
         xi = to_host(bt.field(x, i))
         assert relerr(to_host(bt.field(y, i)), O.forward_fft(xi, 2, n, b, p)) < TOL["c64"]
+
+
+def test_timeout_ends_only_its_own_launch():
+    """A barrier timeout aborts only the launch it happened in: a call made after it,
+    before anyone reads the status, still runs every step; the sticky flag then still
+    reports the earlier timeout once, and is cleared."""
+    from stencilfft_b200 import abi
+    bt = _batch(MIXED[:3], "c64")
+    bt.barrier_probe(1)                           # times out (2 s), flag left set
+    x, y = bt.empty(), bt.empty()
+    bt.fill(x, abi.ZM_FIELD_GAUSSIAN, 2)
+    bt.forward_fft(x, y)
+    for i, (n, b, p) in enumerate(MIXED[:3]):
+        xi = to_host(bt.field(x, i))
+        assert relerr(to_host(bt.field(y, i)), O.forward_fft(xi, 2, n, b, p)) < TOL["c64"]
+    assert bt.status() == 1
+    assert bt.status() == 0
