@@ -158,3 +158,59 @@ def test_c1_stated_field_against_reference_and_oracle():
     nat_lap = (np.roll(nat, 1, 0) + np.roll(nat, -1, 0) + np.roll(nat, 1, 1) + np.roll(nat, -1, 1)
                - 4 * nat)
     assert relerr(O.real_layout_to_natural(lap_ref, 2, n, b, p), nat_lap) < 1e-14
+
+
+TIMING = [(2, 1024, 32, 2), (2, 4096, 32, 4), (3, 256, 16, 4)]
+
+
+@pytest.mark.parametrize("dim,n,b,p", TIMING)
+def test_reference_pipeline_timing(dim, n, b, p):
+    """The GPU-vs-GPU bar: the reference's own pipeline (cuFFT + its kernels, all virtual
+    ranks on this GPU, host-staged exchanges as it ships and, where built, the
+    __GPU__AWARE__MPI__ form) against the library on the same field.  Reference times are
+    barrier to barrier per call (its TOTAL timer, fft.cu:202-338); the library's are CUDA
+    events over 10 calls.  Prints one JSON line per configuration; the parity of the two
+    outputs is asserted."""
+    import json
+    import torch
+    from stencilfft_b200 import Plan, abi
+    ref = _ref(n, b, p)
+    pl128 = Plan(dim, n, b, p, dtype="c128")
+    u = pl128.empty()
+    pl128.fill(u, abi.ZM_FIELD_GAUSSIAN, 2)
+    buf = to_host(u)
+    row = {"dim": dim, "n": n, "b": b, "p": p, "ranks": p ** dim}
+    for aware in (False, True):
+        if not R.available(n, b, p, aware):
+            continue
+        r = R.RefPipeline(n, b, p, aware)
+        tag = "ref_aware" if aware else "ref_staged"
+        spec, ms_f, log = r.fft(buf, dim, reps=2)
+        _, ms_i, _ = r.fft(spec, dim, inverse=True, scale=1.0 / n ** dim, reps=2)
+        lap, ms_l, _ = r.laplace(buf, dim, reps=2)
+        row[tag] = {"fwd_ms": round(ms_f, 3), "inv_ms": round(ms_i, 3), "laplace_ms": round(ms_l, 3),
+                    "stages_ns": {k: v[-1] for k, v in R.stage_times(log).items()}}
+    for dt in ("c128", "c64"):
+        pl = pl128 if dt == "c128" else Plan(dim, n, b, p, dtype=dt)
+        x = u if dt == "c128" else u.to(torch.complex64)
+        y, w, z = pl.empty(), pl.empty(), pl.empty()
+
+        def t(fn, reps=10):
+            fn()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / reps
+        ms_f = t(lambda: pl.forward_fft(x, y, work=w))
+        ms_i = t(lambda: pl.inverse_fft(y, z, scale=1.0 / n ** dim, work=w))
+        ms_l = t(lambda: pl.laplace(x, z, inv_h2=1.0))
+        row[dt] = {"fwd_ms": round(ms_f, 4), "inv_ms": round(ms_i, 4), "laplace_ms": round(ms_l, 4)}
+        if dt == "c128":
+            pl.forward_fft(x, y, work=w)
+            assert relerr(to_host(y), spec) < 1e-12
+            pl.laplace(x, z, inv_h2=1.0)
+            assert relerr(to_host(z), lap) < 1e-15
+    print("\nREFTIMING " + json.dumps(row))
