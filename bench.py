@@ -468,6 +468,47 @@ def run_profile_case(args):
     `ncu -k ... -s/-c` captures."""
     import torch
     from stencilfft_b200 import Plan, abi
+    if args.profile_ops == "fft3d":
+        # 3D forward + inverse transform with a workspace, N = 512, P = 4, B = 32 (1 GiB per
+        # c64 field, three fields)
+        n3 = 512
+        pl3 = Plan(3, n3, 32, P, dtype=args.profile_dtype)
+        u3, s3, w3 = pl3.empty(), pl3.empty(), pl3.empty()
+        pl3.fill(u3, abi.ZM_FIELD_GAUSSIAN, 2)
+        for _ in range(2):
+            pl3.forward_fft(u3, s3, work=w3)
+            pl3.inverse_fft(s3, u3, scale=1.0 / n3 ** 3, work=w3)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": {"dim": 3, "n": n3, "p": P, "b": 32, "dtype": args.profile_dtype,
+                                           "ops": "fft3d", "field_bytes": pl3.field_bytes}}))
+        return
+    if args.profile_ops == "batch":
+        # the 96-field Poisson batch (32 x 256^2, 32 x 512^2, 24 x 1024^2, 8 x 2048^2; P = 2,
+        # B = N / 8), two calls
+        from stencilfft_b200 import Batch
+        sizes = [256] * 32 + [512] * 32 + [1024] * 24 + [2048] * 8
+        bt = Batch(sizes, [n // 8 for n in sizes], [2] * len(sizes), dtype=args.profile_dtype)
+        rhs, phi, res, work = bt.empty(), bt.empty(), bt.empty(), bt.empty()
+        bt.fill(rhs, abi.ZM_FIELD_GAUSSIAN, 100)
+        for _ in range(2):
+            bt.poisson(rhs, phi, res, work, length=1.0)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": {"ops": "batch", "fields": len(sizes), "dtype": args.profile_dtype,
+                                           "elems": bt.total}}))
+        return
+    if args.profile_ops == "layout":
+        # natural -> interleaved converter and a reciprocal-space pointwise operator, N = 8192
+        n = args.profile_n
+        pl = Plan(2, n, B, P, dtype=args.profile_dtype)
+        nat, buf = pl.empty(), pl.empty()
+        pl.fill(nat, abi.ZM_FIELD_GAUSSIAN, 3)
+        for _ in range(2):
+            pl.natural_to_real(nat, buf)
+            pl.spectral_apply(buf, abi.ZM_SPECTRAL_GAUSSIAN, n / 16)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": {"n": n, "p": P, "b": B, "dtype": args.profile_dtype,
+                                           "ops": "layout", "field_bytes": pl.field_bytes}}))
+        return
     if args.profile_ops == "lap3d":
         # 3D 7-point Laplacian, N = 512, P = 4, B = 32 (1 GiB per c64 field, two fields)
         n3 = 512
@@ -525,7 +566,8 @@ def main():
                     help="run the small profiling case only (for ncu captures)")
     ap.add_argument("--profile-n", type=int, default=8192)
     ap.add_argument("--profile-dtype", default="c64")
-    ap.add_argument("--profile-ops", choices=["all", "fwd", "inv", "lap3d"], default="all")
+    ap.add_argument("--profile-ops", choices=["all", "fwd", "inv", "lap3d", "fft3d", "batch", "layout"],
+                    default="all")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.profile_case:
