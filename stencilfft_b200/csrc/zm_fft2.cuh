@@ -112,7 +112,12 @@ template <int LV, int LM, int CL, int TL, int NT> struct SliceGeom {
     static constexpr bool PADX = RA2 > 1;
     static constexpr int XR = PADX ? VEC + RA2 : VEC + 2;
     static constexpr int YP = VEC <= 4 ? 1 : 0;              // pad per 16 in a column
-    static constexpr int YR = VEC <= 4 ? M + M / 16 : M + 1; // padded column
+    // padded column; for VEC <= 4 the column stages run with lanes over (VL columns) x
+    // (16 / VL consecutive points), so the column stride is rounded up to 16 / VL (mod 16,
+    // in 8-byte words of complex64) to keep those 16 lanes on 16 distinct bank pairs
+    static constexpr int YR0 = M + M / 16;
+    static constexpr int YRES = VL >= 16 ? 0 : 16 / VL;
+    static constexpr int YR = VEC <= 4 ? YR0 + (((YRES - YR0) % 16) + 16) % 16 : M + 1;
     static constexpr int XE = TL * ML * XR, YE = TL * VL * YR;
     static constexpr int ELEMS = XE > YE ? XE : YE;
     static ZM_DEV int X(int t, int n1l, int p) { return (t * ML + n1l) * XR + p + (PADX ? p / RA1 : 0); }
@@ -642,8 +647,17 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
                 const int u = tid + i * NT;
                 un1[i] = u % ML;
                 ut[i] = u / ML;
+                if constexpr ((RA1 * sizeof(C)) % 16 == 0 && (SG::XR * sizeof(C)) % 16 == 0) {
+                    // the row as 16-byte vectors: lanes on consecutive rows of XR = VEC + 2
+                    // points take distinct bank groups (8-byte reads of the same rows collide)
+                    const uint4 *rp = reinterpret_cast<const uint4 *>(&S[SG::X(ut[i], un1[i], 0)]);
 #pragma unroll
-                for (int r = 0; r < RA1; r++) v[i][r] = S[SG::X(ut[i], un1[i], r)];
+                    for (int q = 0; q < RA1 * (int)sizeof(C) / 16; q++)
+                        *reinterpret_cast<uint4 *>(&v[i][q * 16 / (int)sizeof(C)]) = rp[q];
+                } else {
+#pragma unroll
+                    for (int r = 0; r < RA1; r++) v[i][r] = S[SG::X(ut[i], un1[i], r)];
+                }
             }
 #pragma unroll
             for (int i = 0; i < NU; i++) dft<RA1, DIR, T>(v[i]);

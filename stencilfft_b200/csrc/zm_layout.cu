@@ -12,21 +12,49 @@
 
 namespace zm {
 
+// Each thread moves CEPT consecutive interleaved elements e: their CEPT gathers (or
+// scatters) on the natural side are all in flight before the first use, and the
+// interleaved side moves as 16-byte vectors.  (One element per thread kept one 8-byte
+// load in flight and waited on it.)  total is a multiple of CEPT (N^dim, N >= 4).
+constexpr int CEPT = 4;
+// CEPT consecutive elements at a CEPT-aligned index, as 16-byte vectors
+template <typename T> ZM_DEV void ld_run(const cpx<T> *p, cpx<T> *v) {
+    constexpr int NV = CEPT * (int)sizeof(cpx<T>) / 16;
+#pragma unroll
+    for (int q = 0; q < NV; q++)
+        reinterpret_cast<uint4 *>(v)[q] = __ldg(reinterpret_cast<const uint4 *>(p) + q);
+}
+template <typename T> ZM_DEV void st_run(cpx<T> *p, const cpx<T> *v) {
+    constexpr int NV = CEPT * (int)sizeof(cpx<T>) / 16;
+#pragma unroll
+    for (int q = 0; q < NV; q++) reinterpret_cast<uint4 *>(p)[q] = reinterpret_cast<const uint4 *>(v)[q];
+}
 template <typename T, bool RECIP, bool TO_NAT>
-__global__ void convert_kernel(const cpx<T> *__restrict__ in, cpx<T> *__restrict__ out, const Geom g,
-                               int64_t total) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= total) return;
-    const int64_t gi = RECIP ? recip_gidx(e, g) : real_gidx(e, g);
-    if (TO_NAT) out[gi] = ldg(in + e);
-    else out[e] = ldg(in + gi);
+__global__ void __launch_bounds__(256) convert_kernel(const cpx<T> *__restrict__ in, cpx<T> *__restrict__ out,
+                                                      const Geom g, int64_t total) {
+    const int64_t e0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * CEPT;
+    if (e0 >= total) return;
+    int64_t gi[CEPT];
+#pragma unroll
+    for (int i = 0; i < CEPT; i++) gi[i] = RECIP ? recip_gidx(e0 + i, g) : real_gidx(e0 + i, g);
+    cpx<T> v[CEPT];
+    if (TO_NAT) {
+        ld_run(in + e0, v);
+#pragma unroll
+        for (int i = 0; i < CEPT; i++) out[gi[i]] = v[i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < CEPT; i++) v[i] = ldg(in + gi[i]);
+        st_run(out + e0, v);
+    }
 }
 
 template <typename T>
 static cudaError_t conv_t(const zm_plan_s *p, bool recip, bool to_nat, const void *in, void *out,
                           cudaStream_t st) {
     const int threads = 256;
-    const unsigned grid = (unsigned)((p->total + threads - 1) / threads);
+    const int64_t nthr = p->total / CEPT;
+    const unsigned grid = (unsigned)((nthr + threads - 1) / threads);
     const cpx<T> *i = reinterpret_cast<const cpx<T> *>(in);
     cpx<T> *o = reinterpret_cast<cpx<T> *>(out);
     if (recip) {
@@ -47,28 +75,39 @@ cudaError_t launch_convert(const zm_plan_s *p, bool reciprocal, bool to_natural,
 }
 
 // --------------------------------------------------------- spectral operators
+// Each thread scales CEPT consecutive elements.  The multiplier is computed in the
+// working precision: FP64 for complex128; FP32 for complex64, where its relative error
+// (a few ulp of FP32) stays far inside the complex64 bar, and the FP64 exp / division
+// made the kernel issue bound.
 template <typename T>
-__global__ void spectral_kernel(cpx<T> *__restrict__ d, const Geom g, int64_t total, int op, double a) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= total) return;
-    int64_t k0, k1, k2;
-    recip_k(e, g, k0, k1, k2);
+__global__ void __launch_bounds__(256) spectral_kernel(cpx<T> *__restrict__ d, const Geom g, int64_t total, int op,
+                                                       double a) {
+    const int64_t e0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * CEPT;
+    if (e0 >= total) return;
+    cpx<T> v[CEPT];
+    ld_run(d + e0, v);
     const int64_t half = g.n >> 1;
-    const double s0 = (double)(k0 >= half ? k0 - g.n : k0);
-    const double s1 = (double)(k1 >= half ? k1 - g.n : k1);
-    const double s2 = (double)(k2 >= half ? k2 - g.n : k2);
-    const double k2sum = s0 * s0 + s1 * s1 + s2 * s2;
-    double f;
-    if (op == 0) f = exp(-k2sum / (2.0 * a * a));
-    else if (op == 1) f = k2sum == 0.0 ? 0.0 : -1.0 / (a * a * k2sum);
-    else f = a;
-    cpx<T> v = d[e];
-    d[e] = {(T)(v.x * f), (T)(v.y * f)};
+    const T inv2a2 = (T)(1.0 / (2.0 * a * a)), inva2 = (T)(1.0 / (a * a)), ta = (T)a;
+#pragma unroll
+    for (int i = 0; i < CEPT; i++) {
+        int64_t k0, k1, k2;
+        recip_k(e0 + i, g, k0, k1, k2);
+        const int64_t s0 = k0 >= half ? k0 - g.n : k0;
+        const int64_t s1 = k1 >= half ? k1 - g.n : k1;
+        const int64_t s2 = k2 >= half ? k2 - g.n : k2;
+        const T k2sum = (T)(s0 * s0 + s1 * s1 + s2 * s2);   // exact in FP64; one rounding in FP32
+        T f;
+        if (op == 0) f = exp(-k2sum * inv2a2);
+        else if (op == 1) f = k2sum == (T)0 ? (T)0 : -inva2 / k2sum;
+        else f = ta;
+        v[i] = {v[i].x * f, v[i].y * f};
+    }
+    st_run(d + e0, v);
 }
 
 cudaError_t launch_spectral(const zm_plan_s *p, void *data, int op, double a, cudaStream_t st) {
     const int threads = 256;
-    const unsigned grid = (unsigned)((p->total + threads - 1) / threads);
+    const unsigned grid = (unsigned)((p->total / CEPT + threads - 1) / threads);
     if (p->dtype == 0)
         spectral_kernel<double><<<grid, threads, 0, st>>>(reinterpret_cast<cpx<double> *>(data), p->g,
                                                           p->total, op, a);

@@ -104,3 +104,24 @@ def test_laplace3d_warp_assignment_covers_each_vector_once(L, K, RX):
         pos = (v0 + 32 * x) * K
         w = pos.reshape(-1, 32)
         assert (np.diff(w, axis=1) == K).all() and (w[:, -1] < L).all()
+
+
+@pytest.mark.parametrize("n,b,p", CONFIGS)
+def test_laplace3d_global_line_order_is_a_permutation(n, b, p):
+    """The complex128 form of the kernel walks lines in global order (global depth, global
+    row, then the P ranks of that row): the map from that order to (rank * L + ld) * L + lr
+    visits every line of every rank once."""
+    L = n // p
+    logB, logP, logL, logN = lg(b), lg(p), lg(L), lg(n)
+    gline = np.arange(p * n * n, dtype=np.int64)
+    cid = gline & (p - 1)
+    gr, gd = (gline >> logP) & (n - 1), gline >> (logP + logN)
+
+    def g2l(gi):
+        return (gi >> logB) & (p - 1), ((gi >> (logB + logP)) << logB) + (gi & (b - 1))
+
+    rid, lr = g2l(gr)
+    did, ld = g2l(gd)
+    rank = (did * p + rid) * p + cid
+    line = (((rank << logL) + ld) << logL) + lr
+    assert np.array_equal(np.sort(line), np.arange(p ** 3 * L * L))
