@@ -64,18 +64,19 @@ def read_peaks():
 
 
 def read_traffic(key: str):
-    """Per-launch DRAM bytes of a kernel from the committed ncu summary (profiles/traffic.txt)."""
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary (profiles/traffic.txt):
+    (bytes, source) -- the value is that capture's, not a measurement of this run."""
     p = ROOT / "profiles" / "traffic.txt"
     if not p.exists():
-        return None
+        return None, None
     for line in p.read_text().splitlines():
         parts = line.split()
         if len(parts) >= 2 and parts[0] == key:
             try:
-                return float(parts[1])
+                return float(parts[1]), "profiles/" + parts[2] if len(parts) > 2 else "profiles/traffic.txt"
             except ValueError:
-                return None
-    return None
+                return None, None
+    return None, None
 
 
 class ClockSampler:
@@ -415,7 +416,7 @@ def run_ours(args, rank: int, world: int):
     # per forward call: x pass persistent, y pass one line per CTA)
     t_launch = main["stage_ms"]["fwd"] / 2
     achieved = (2 * F) / (t_launch * 1e-3) / 1e9
-    traffic = read_traffic("k3_pass_fwd_c64_N16384")
+    traffic, traffic_src = read_traffic("k3_pass_fwd_c64_N16384")
     fft_flops = 5.0 * N * N * math.log2(N * N)
     # algorithmic bytes: 4F per 2D transform, 2F per stencil (6F for the three fused
     # stencils, which move 4F: one read, three writes)
@@ -440,7 +441,8 @@ def run_ours(args, rank: int, world: int):
         "roofline": {"bound": "hbm", "kernel": "k3_pass_kernel<6,8,fwd> (x pass persistent, y pass one line per CTA)",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                     "traffic": traffic, "algorithmic_bytes_per_launch": 2 * F},
+                     "traffic": traffic, "traffic_source": f"committed ncu capture ({traffic_src})",
+                     "algorithmic_bytes_per_launch": 2 * F},
         "stages": stages,
         "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": main["h2d"],
                 "d2h_bytes_per_step": main["d2h"], "steps": main["e2e_steps"],

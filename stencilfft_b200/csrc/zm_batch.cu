@@ -138,31 +138,69 @@ ZM_DEV int64_t real_elem(int64_t gr, int64_t gc, const Geom &g) {
     return (((rid << g.logP) + cid) << (2 * g.logL)) + (lr << g.logL) + pos;
 }
 
-// Both sub-transforms of a tile: compile-time-sized stages for the complex64 tiles with
-// VEC = 4 (the layout the B autotuner picks for the batch sizes, B = N / 8 at P = 2) and
-// M = 16 .. 1024; the runtime-sized stages for every other shape.
-template <typename T, int EPT, bool INV, int LM>
+// Both sub-transforms of a tile: compile-time-sized stages (LMC = log2 M) for the
+// complex64 tiles with VEC = 4 (the layout the B autotuner picks for the batch sizes, B =
+// N / 8 at P = 2), or the runtime-sized stages (LMC = 0) for every other shape.
+template <typename T, int EPT, bool INV, int LM, typename SW>
 __device__ __noinline__ void tile_transform_v4(cpx<T> *s, int tid, const tw<T> *twN) {
-    tile_transform_ct<T, EPT, INV, 2, LM, kBatchThreads>(s, tid, twN);
+    tile_transform_ct<T, EPT, INV, 2, LM, kBatchThreads, SW>(s, tid, twN);
 }
-template <typename T, int EPT, bool INV>
+template <typename T, int EPT, bool INV, int LMC, typename SW>
 ZM_DEV void batch_tile_transform(cpx<T> *s, const BatchField &f, int nthr, int tid, const tw<T> *twN) {
-    const Geom &g = f.g;
-    if constexpr (sizeof(T) == 4 && EPT == 16) {
-        if (g.logVEC == 2) {
-            switch (g.logM) {
-            case 4: return tile_transform_v4<T, EPT, INV, 4>(s, tid, twN);
-            case 5: return tile_transform_v4<T, EPT, INV, 5>(s, tid, twN);
-            case 6: return tile_transform_v4<T, EPT, INV, 6>(s, tid, twN);
-            case 7: return tile_transform_v4<T, EPT, INV, 7>(s, tid, twN);
-            case 8: return tile_transform_v4<T, EPT, INV, 8>(s, tid, twN);
-            case 9: return tile_transform_v4<T, EPT, INV, 9>(s, tid, twN);
-            case 10: return tile_transform_v4<T, EPT, INV, 10>(s, tid, twN);
-            default: break;
-            }
-        }
+    if constexpr (LMC > 0) {
+        tile_transform_v4<T, EPT, INV, LMC, SW>(s, tid, twN);
+    } else {
+        const Geom &g = f.g;
+        tile_transform<T, EPT, INV>(s, g, f.rad_vec, f.nst_vec, f.rad_m, f.nst_m, nthr, tid, twN);
     }
-    tile_transform<T, EPT, INV>(s, g, f.rad_vec, f.nst_vec, f.rad_m, f.nst_m, nthr, tid, twN);
+}
+
+// One tile of an axis-pass step: load, transform(s), store.  SW is the shared-memory
+// slot permutation of the tile (SwzV4 for the compile-time VEC = 4 tiles).
+template <typename T, int EPT, int LMC, typename SW>
+__device__ __noinline__ void batch_tile(int op, bool scale, double a, const BatchField &sf, const Tile c, cpx<T> *s,
+                                        const cpx<T> *in, cpx<T> *out, int64_t l0, int nthr, int tid) {
+    const Geom &g = sf.g;
+    const tw<T> *twN = reinterpret_cast<const tw<T> *>(sf.twN);
+    const bool xpass = op == BOP_X_FWD || op == BOP_X_INV;
+    if (op == BOP_X_FWD || op == BOP_Y_FWD) {
+        tile_load_vec<EPT, SW>(c, g, s, in, nthr, tid);
+        __syncthreads();
+        batch_tile_transform<T, EPT, false, LMC, SW>(s, sf, nthr, tid, twN);
+        tile_store_freq<EPT, SW>(c, g, s, out, false, (T)1, (T)0, nthr, tid);
+    } else if (op == BOP_X_INV || op == BOP_Y_INV) {
+        tile_load_freq<EPT, SW>(c, g, s, in, nthr, tid);
+        __syncthreads();
+        batch_tile_transform<T, EPT, true, LMC, SW>(s, sf, nthr, tid, twN);
+        const bool scl = scale && xpass;
+        const T sc = (T)(1.0 / ((double)g.n * (double)g.n));
+        tile_store_vec<EPT, SW>(c, g, s, out, scl, sc, (T)0, nthr, tid);
+    } else {   // BOP_Y_POISSON
+        tile_load_vec<EPT, SW>(c, g, s, in, nthr, tid);
+        __syncthreads();
+        batch_tile_transform<T, EPT, false, LMC, SW>(s, sf, nthr, tid, twN);
+        // slot (t, k1, k2) holds the frequency the y pass would store at rank
+        // (rid = k2 / VP, cid), local row p, column pos = k1 VP + k2 % VP
+        // (reciprocal_to_global, utils.h:265-268)
+        const int tot = sf.T << g.logN;
+        const double a2 = a * a;
+        for (int e = tid; e < tot; e += nthr) {
+            const int t = e >> g.logN, r = e & (int)(g.n - 1);
+            const int k1 = r >> g.logVEC, k2 = r & (int)(g.vec - 1);
+            const int64_t rid = k2 >> g.logVP;
+            const int64_t pos = ((int64_t)k1 << g.logVP) + (k2 & (int)(g.vp - 1));
+            const int64_t l = l0 + t, cid = l >> g.logL, p = l & (g.L - 1);
+            const double sa = sfreq(d_ct(cid * g.L + d_lp(p, g), g), g);
+            const double sb = sfreq(d_ct(rid * g.L + d_lp(pos, g), g), g);
+            const double ksq = sa * sa + sb * sb;
+            const double fac = ksq == 0.0 ? 0.0 : -1.0 / (a2 * ksq);
+            const cpx<T> v = s[SW::f(e)];
+            s[SW::f(e)] = {(T)(v.x * fac), (T)(v.y * fac)};
+        }
+        __syncthreads();
+        batch_tile_transform<T, EPT, true, LMC, SW>(s, sf, nthr, tid, twN);
+        tile_store_vec<EPT, SW>(c, g, s, out, false, (T)1, (T)0, nthr, tid);
+    }
 }
 
 template <typename T, int EPT>
@@ -277,45 +315,26 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batch_kernel(const BatchPara
             __syncthreads();
             const cpx<T> *in = reinterpret_cast<const cpx<T> *>(S.in) + sf.off;
             cpx<T> *out = reinterpret_cast<cpx<T> *>(S.out) + sf.off;
-            const tw<T> *twN = reinterpret_cast<const tw<T> *>(sf.twN);
-            if (S.op == BOP_X_FWD || S.op == BOP_Y_FWD) {
-                tile_load_vec<EPT>(c, g, s, in, nthr, tid);
-                __syncthreads();
-                batch_tile_transform<T, EPT, false>(s, sf, nthr, tid, twN);
-                tile_store_freq<EPT>(c, g, s, out, false, (T)1, (T)0, nthr, tid);
-            } else if (S.op == BOP_X_INV || S.op == BOP_Y_INV) {
-                tile_load_freq<EPT>(c, g, s, in, nthr, tid);
-                __syncthreads();
-                batch_tile_transform<T, EPT, true>(s, sf, nthr, tid, twN);
-                const bool scl = S.scale && xpass;
-                const T sc = (T)(1.0 / ((double)g.n * (double)g.n));
-                tile_store_vec<EPT>(c, g, s, out, scl, sc, (T)0, nthr, tid);
-            } else {   // BOP_Y_POISSON
-                tile_load_vec<EPT>(c, g, s, in, nthr, tid);
-                __syncthreads();
-                batch_tile_transform<T, EPT, false>(s, sf, nthr, tid, twN);
-                // slot (t, k1, k2) holds the frequency the y pass would store at rank
-                // (rid = k2 / VP, cid), local row p, column pos = k1 VP + k2 % VP
-                // (reciprocal_to_global, utils.h:265-268)
-                const int tot = sf.T << g.logN;
-                const double a2 = S.a * S.a;
-                for (int e = tid; e < tot; e += nthr) {
-                    const int t = e >> g.logN, r = e & (int)(g.n - 1);
-                    const int k1 = r >> g.logVEC, k2 = r & (int)(g.vec - 1);
-                    const int64_t rid = k2 >> g.logVP;
-                    const int64_t pos = ((int64_t)k1 << g.logVP) + (k2 & (int)(g.vp - 1));
-                    const int64_t l = l0 + t, cid = l >> g.logL, p = l & (g.L - 1);
-                    const double sa = sfreq(d_ct(cid * g.L + d_lp(p, g), g), g);
-                    const double sb = sfreq(d_ct(rid * g.L + d_lp(pos, g), g), g);
-                    const double ksq = sa * sa + sb * sb;
-                    const double fac = ksq == 0.0 ? 0.0 : -1.0 / (a2 * ksq);
-                    const cpx<T> v = s[e];
-                    s[e] = {(T)(v.x * fac), (T)(v.y * fac)};
+            // SwzV4<S>: S = 2 + log2 of the first column stage's radix (radix_sched)
+#define ZM_BT(LMC, SS) batch_tile<T, EPT, LMC, SwzV4<SS>>(S.op, S.scale != 0, S.a, sf, c, s, in, out, l0, nthr, tid)
+            bool done = false;
+            if constexpr (sizeof(T) == 4 && EPT == 16) {
+                if (g.logVEC == 2) {
+                    done = true;
+                    switch (g.logM) {
+                    case 4: ZM_BT(4, 6); break;
+                    case 5: ZM_BT(5, 6); break;
+                    case 6: ZM_BT(6, 4); break;
+                    case 7: ZM_BT(7, 5); break;
+                    case 8: ZM_BT(8, 6); break;
+                    case 9: ZM_BT(9, 3); break;
+                    case 10: ZM_BT(10, 4); break;
+                    default: done = false; break;
+                    }
                 }
-                __syncthreads();
-                batch_tile_transform<T, EPT, true>(s, sf, nthr, tid, twN);
-                tile_store_vec<EPT>(c, g, s, out, false, (T)1, (T)0, nthr, tid);
             }
+#undef ZM_BT
+            if (!done) batch_tile<T, EPT, 0, SwzNone>(S.op, S.scale != 0, S.a, sf, c, s, in, out, l0, nthr, tid);
         }
     }
 }

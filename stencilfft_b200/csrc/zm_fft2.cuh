@@ -121,7 +121,15 @@ template <int LV, int LM, int CL, int TL, int NT> struct SliceGeom {
     static constexpr int XE = TL * ML * XR, YE = TL * VL * YR;
     static constexpr int ELEMS = XE > YE ? XE : YE;
     static ZM_DEV int X(int t, int n1l, int p) { return (t * ML + n1l) * XR + p + (PADX ? p / RA1 : 0); }
-    static ZM_DEV int Y(int t, int k2l, int q) { return (t * VL + k2l) * YR + q + (q >> 4) * YP; }
+    // Column position swizzle for VEC <= 4 tiles of several lines: where lanes run over the
+    // lines t first (a strided frequency side), lines t and t + 4 would sit on the same bank
+    // pairs (their rows are 4 YR = 0 mod 16 words apart); q ^ ysw(t) spreads the eight
+    // lines of a half-warp over the two quads of 16 that the second column (+ 4) leaves
+    // free, and is a constant permutation inside each aligned 16 for every other access.
+    static constexpr bool YSW = VEC <= 4 && TL >= 2;
+    static_assert(!YSW || M >= 16, "swizzle stays inside an aligned run of 16 points");
+    static ZM_DEV int ysw(int t) { return YSW ? ((t & 3) | (((t >> 2) & 1) << 3)) : 0; }
+    static ZM_DEV int Y(int t, int k2l, int q) { return (t * VL + k2l) * YR + (q ^ ysw(t)) + (q >> 4) * YP; }
     // staging rows of the persistent forward pass: one row of sg interleaved lines
     // (sg VEC points, a bulk copy each); the stride keeps the first row stage's reads
     // (lanes over sg lines x RA2 points, then rows) free of bank conflicts

@@ -13,6 +13,20 @@
 
 namespace zm {
 
+// Physical slot of tile element i in shared memory.  SwzNone: the element itself.
+// SwzV4<S> (tiles with VEC = 4): i ^ (i >> 4 & 3) ^ ((i >> S & 3) << 2), a permutation
+// inside every aligned run of 16 elements, chosen so that the 16 lanes of a half-warp
+// hit 16 distinct bank pairs in every stage: the row stage (lanes on rows 4 elements
+// apart), the first column stage's Stockham writes (lanes on units 4 R elements apart,
+// S = 2 + log2 R) and contiguous runs (unchanged).  Without it those accesses were 4-way
+// conflicted.
+struct SwzNone {
+    static ZM_DEV int f(int i) { return i; }
+};
+template <int S> struct SwzV4 {
+    static ZM_DEV int f(int i) { return i ^ ((i >> 4) & 3) ^ (((i >> S) & 3) << 2); }
+};
+
 // ------------------------------------------------------------ Stockham stage
 // One radix-R stage over all sub-transforms of length n held in shared memory.
 //   COLM = false: sub-transform (t, n1) is the contiguous row s[t*N + n1*VEC + i]
@@ -120,7 +134,8 @@ ZM_DEV void tile_transform(cpx<T> *s, const Geom &g, const int *rad_vec, int nst
 // arithmetic in the same order.
 constexpr int ct_log2(int x) { return x <= 1 ? 0 : 1 + ct_log2(x >> 1); }
 
-template <int R, int EPT, bool COLM, int DIR, bool PRETW, typename T, int LV, int LM, int LN, int NS, int NT>
+template <int R, int EPT, bool COLM, int DIR, bool PRETW, typename T, int LV, int LM, int LN, int NS, int NT,
+          typename SW = SwzNone>
 ZM_DEV void stockham_stage_ct(cpx<T> *s, int tid, const tw<T> *twN) {
     constexpr int NB = EPT / R;
     constexpr bool CONJ = DIR > 0;
@@ -153,7 +168,7 @@ ZM_DEV void stockham_stage_ct(cpx<T> *s, int tid, const tw<T> *twN) {
 #pragma unroll
         for (int r = 0; r < R; r++) {
             const int i = j + r * nR;
-            cpx<T> x = s[bb + i * str];
+            cpx<T> x = s[SW::f(bb + i * str)];
             if constexpr (PRETW) x = twmul<CONJ>(x, ldtw(twN, (int64_t)i * tagn));
             v[u][r] = x;
         }
@@ -171,7 +186,7 @@ ZM_DEV void stockham_stage_ct(cpx<T> *s, int tid, const tw<T> *twN) {
         dft<R, DIR, T>(v[u]);
         const int idxD = (j - k) * R + k;
 #pragma unroll
-        for (int r = 0; r < R; r++) s[base[u] + (idxD + r * NS) * str] = v[u][r];
+        for (int r = 0; r < R; r++) s[SW::f(base[u] + (idxD + r * NS) * str)] = v[u][r];
     }
     __syncthreads();
 }
@@ -182,25 +197,26 @@ template <int LN, int RL> struct radix_sched {
     static constexpr int rad(int i) { return (rem && i == 0) ? (1 << rem) : (1 << RL); }
 };
 
-template <int ST, int NS, int EPT, bool COLM, int DIR, bool PRE, typename T, int LV, int LM, int LN, int NT, int RL>
+template <int ST, int NS, int EPT, bool COLM, int DIR, bool PRE, typename T, int LV, int LM, int LN, int NT, int RL,
+          typename SW = SwzNone>
 ZM_DEV void run_subfft_ct(cpx<T> *s, int tid, const tw<T> *twN) {
     using SC = radix_sched<LN, RL>;
     if constexpr (ST < SC::nst) {
         constexpr int R = SC::rad(ST);
-        stockham_stage_ct<R, EPT, COLM, DIR, PRE && ST == 0, T, LV, LM, LN, NS, NT>(s, tid, twN);
-        run_subfft_ct<ST + 1, NS * R, EPT, COLM, DIR, PRE, T, LV, LM, LN, NT, RL>(s, tid, twN);
+        stockham_stage_ct<R, EPT, COLM, DIR, PRE && ST == 0, T, LV, LM, LN, NS, NT, SW>(s, tid, twN);
+        run_subfft_ct<ST + 1, NS * R, EPT, COLM, DIR, PRE, T, LV, LM, LN, NT, RL, SW>(s, tid, twN);
     }
 }
 
-template <typename T, int EPT, bool INV, int LV, int LM, int NT>
+template <typename T, int EPT, bool INV, int LV, int LM, int NT, typename SW = SwzNone>
 ZM_DEV void tile_transform_ct(cpx<T> *s, int tid, const tw<T> *twN) {
     constexpr int RL = EPT >= 16 ? 4 : 3;   // radix_schedule(n, EPT): largest radix EPT
     if constexpr (!INV) {
-        run_subfft_ct<0, 1, EPT, false, -1, false, T, LV, LM, LV, NT, RL>(s, tid, twN);
-        run_subfft_ct<0, 1, EPT, true, -1, true, T, LV, LM, LM, NT, RL>(s, tid, twN);
+        run_subfft_ct<0, 1, EPT, false, -1, false, T, LV, LM, LV, NT, RL, SW>(s, tid, twN);
+        run_subfft_ct<0, 1, EPT, true, -1, true, T, LV, LM, LM, NT, RL, SW>(s, tid, twN);
     } else {
-        run_subfft_ct<0, 1, EPT, true, 1, false, T, LV, LM, LM, NT, RL>(s, tid, twN);
-        run_subfft_ct<0, 1, EPT, false, 1, true, T, LV, LM, LV, NT, RL>(s, tid, twN);
+        run_subfft_ct<0, 1, EPT, true, 1, false, T, LV, LM, LM, NT, RL, SW>(s, tid, twN);
+        run_subfft_ct<0, 1, EPT, false, 1, true, T, LV, LM, LV, NT, RL, SW>(s, tid, twN);
     }
 }
 
@@ -261,7 +277,7 @@ ZM_DEV int tile_freq_slot(const Geom &g, int t, int ch, int pos) {
 // few bytes in flight to cover the DRAM latency.
 
 // vector side -> rows s[t][c*L + pos] = s[t][n1*VEC + n2]
-template <int EPT, typename T>
+template <int EPT, typename SW = SwzNone, typename T>
 ZM_DEV void tile_load_vec(const Tile &c, const Geom &g, cpx<T> *s, const cpx<T> *in, int nthr, int tid) {
     cpx<T> v[EPT];
 #pragma unroll
@@ -273,11 +289,11 @@ ZM_DEV void tile_load_vec(const Tile &c, const Geom &g, cpx<T> *s, const cpx<T> 
         v[i] = ldg(in + c.abase[t] + ch * c.a_chunk + pos);
     }
 #pragma unroll
-    for (int i = 0; i < EPT; i++) s[tid + i * nthr] = v[i];
+    for (int i = 0; i < EPT; i++) s[SW::f(tid + i * nthr)] = v[i];
 }
 
 // frequency side (t, c, pos = k1*VP + f) -> s[t][k1*VEC + c*VP + f]
-template <int EPT, typename T>
+template <int EPT, typename SW = SwzNone, typename T>
 ZM_DEV void tile_load_freq(const Tile &c, const Geom &g, cpx<T> *s, const cpx<T> *in, int nthr, int tid) {
     cpx<T> v[EPT];
 #pragma unroll
@@ -290,24 +306,24 @@ ZM_DEV void tile_load_freq(const Tile &c, const Geom &g, cpx<T> *s, const cpx<T>
     for (int i = 0; i < EPT; i++) {
         int t, ch, pos;
         tile_freq_coords(c, g, tid + i * nthr, t, ch, pos);
-        s[tile_freq_slot(g, t, ch, pos)] = v[i];
+        s[SW::f(tile_freq_slot(g, t, ch, pos))] = v[i];
     }
 }
 
-template <int EPT, typename T>
+template <int EPT, typename SW = SwzNone, typename T>
 ZM_DEV void tile_store_freq(const Tile &c, const Geom &g, const cpx<T> *s, cpx<T> *out, bool scl, T sr,
                             T si, int nthr, int tid) {
 #pragma unroll
     for (int i = 0; i < EPT; i++) {
         int t, ch, pos;
         tile_freq_coords(c, g, tid + i * nthr, t, ch, pos);
-        cpx<T> v = s[tile_freq_slot(g, t, ch, pos)];
+        cpx<T> v = s[SW::f(tile_freq_slot(g, t, ch, pos))];
         if (scl) v = {v.x * sr - v.y * si, v.x * si + v.y * sr};
         out[c.fbase[t] + ch * c.f_chunk + pos * c.f_pos] = v;
     }
 }
 
-template <int EPT, typename T>
+template <int EPT, typename SW = SwzNone, typename T>
 ZM_DEV void tile_store_vec(const Tile &c, const Geom &g, const cpx<T> *s, cpx<T> *out, bool scl, T sr,
                            T si, int nthr, int tid) {
 #pragma unroll
@@ -316,7 +332,7 @@ ZM_DEV void tile_store_vec(const Tile &c, const Geom &g, const cpx<T> *s, cpx<T>
         const int t = e >> g.logN;
         const int r = e & (int)(g.n - 1);
         const int ch = r >> g.logL, pos = r & (int)(g.L - 1);
-        cpx<T> v = s[e];
+        cpx<T> v = s[SW::f(e)];
         if (scl) v = {sr * v.x - si * v.y, sr * v.y + si * v.x};
         out[c.abase[t] + ch * c.a_chunk + pos] = v;
     }

@@ -24,3 +24,18 @@ def to_dev(x: np.ndarray, dtype: str):
 
 def to_host(t) -> np.ndarray:
     return t.detach().cpu().numpy().astype(np.complex128)
+
+
+def ramp_spectrum(dim: int, n: int) -> np.ndarray:
+    """Closed-form DFT of the reference's init_host fixture, x = global linear index
+    (row-major, last axis fastest), in natural order: per axis, the DFT of a constant
+    (S = n at k = 0) and of a ramp 0..n-1 (T = n / (w^k - 1), n(n-1)/2 at k = 0)."""
+    k = np.arange(n)
+    w = np.exp(-2j * np.pi * k / n)
+    S = np.where(k == 0, n, 0).astype(np.complex128)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        T = np.where(k == 0, n * (n - 1) / 2, n / (w - 1))
+    if dim == 2:
+        return n * np.multiply.outer(T, S) + np.multiply.outer(S, T)
+    return (n * n * np.einsum("i,j,k->ijk", T, S, S) + n * np.einsum("i,j,k->ijk", S, T, S)
+            + np.einsum("i,j,k->ijk", S, S, T))

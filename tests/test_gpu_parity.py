@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from helpers import TOL, rand_field, relerr, to_dev, to_host
+from helpers import TOL, ramp_spectrum, rand_field, relerr, to_dev, to_host
 
 pytestmark = pytest.mark.gpu
 
@@ -65,6 +65,25 @@ def test_every_kernel_variant_matches_oracle(dim, n, b, p, dt):
         assert relerr(to_host(d_out), ref) < TOL[dt], v
         pl.inverse_fft(d_out, back, scale=1.0 / n ** dim, work=work)
         assert relerr(to_host(back), buf) < TOL[dt], v
+
+
+@pytest.mark.parametrize("dt", ["c128", "c64"])
+@pytest.mark.parametrize("dim,n,b,p", [(2, 64, 4, 2), (2, 128, 8, 4), (2, 1024, 32, 2), (2, 4096, 64, 4),
+                                       (3, 16, 2, 2), (3, 32, 2, 4), (3, 64, 4, 4)])
+def test_reference_ramp_fixture_known_answer(dim, n, b, p, dt):
+    """The reference's init_host fixture (x = global linear index, zmodel/utils.cu), which
+    the oracle reproduces bit-exactly, through the CUDA forward transform against its
+    closed-form spectrum, and back through the inverse."""
+    import torch
+    buf = O.init_ramp(dim, n, b, p)
+    want = O.natural_to_reciprocal_layout(ramp_spectrum(dim, n), b, p)
+    pl = _plan(dim, n, b, p, dt)
+    d_in = to_dev(buf, dt)
+    d_out, work, back = torch.empty_like(d_in), torch.empty_like(d_in), torch.empty_like(d_in)
+    pl.forward_fft(d_in, d_out, work=work)
+    assert relerr(to_host(d_out), want) < TOL[dt], relerr(to_host(d_out), want)
+    pl.inverse_fft(d_out, back, scale=1.0 / n ** dim, work=work)
+    assert relerr(to_host(back), buf) < TOL[dt]
 
 
 @pytest.mark.parametrize("dim,n,b,p", CFG_2D[:6] + CFG_3D[:3])

@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import oracle as O
+from helpers import ramp_spectrum
 
 # (dim, N, B, P): corners of the reference's run.sh / run3d.sh sweep plus small
 # versions of the benchmark layouts.
@@ -127,16 +128,7 @@ def test_ramp_known_answer(dim, n, b, p):
     """Closed-form spectrum of the reference fixture x = global linear index."""
     buf = O.init_ramp(dim, n, b, p)
     X = O.reciprocal_layout_to_natural(O.forward_fft(buf, dim, n, b, p), dim, n, b, p)
-    k = np.arange(n)
-    w = np.exp(-2j * np.pi * k / n)
-    S = np.where(k == 0, n, 0).astype(np.complex128)
-    with np.errstate(divide="ignore", invalid="ignore"):
-        T = np.where(k == 0, n * (n - 1) / 2, n / (w - 1))
-    if dim == 2:
-        exp = n * np.multiply.outer(T, S) + np.multiply.outer(S, T)
-    else:
-        exp = (n * n * np.einsum("i,j,k->ijk", T, S, S) + n * np.einsum("i,j,k->ijk", S, T, S)
-               + np.einsum("i,j,k->ijk", S, S, T))
+    exp = ramp_spectrum(dim, n)
     assert relerr(X, exp) < 1e-13
 
 
