@@ -493,6 +493,307 @@ __global__ void __launch_bounds__(256) stencil3d_lines_kernel(const S *__restric
     }
 }
 
+// ------------------------------------------------ 3D Laplacian on shared-memory plane tiles
+// mbarrier helpers (bulk copies into shared memory complete on an mbarrier)
+ZM_DEV unsigned st_smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+ZM_DEV void st_mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(st_smem_u32(bar)), "r"(count) : "memory");
+}
+ZM_DEV void st_mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(st_smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+ZM_DEV bool st_mbar_try_wait(uint64_t *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(st_smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+ZM_DEV unsigned long long st_gtimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+ZM_DEV void st_bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     st_smem_u32(dst)),
+                 "l"((unsigned long long)__cvta_generic_to_global(src)), "r"(bytes), "r"(st_smem_u32(bar))
+                 : "memory");
+}
+constexpr unsigned long long kPlaneWaitNs = 1000000000ull;   // 1 s per bounded wait
+constexpr int kMarchSlots = 4;                                // plane tiles in flight + in use
+
+ZM_DEV void st_cp_async(void *dst, const void *src, int bytes) {   // 8 or 16 bytes, aligned
+    if (bytes == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(st_smem_u32(dst)),
+                     "l"((unsigned long long)__cvta_generic_to_global(src))
+                     : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(st_smem_u32(dst)),
+                     "l"((unsigned long long)__cvta_generic_to_global(src))
+                     : "memory");
+}
+ZM_DEV void st_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> ZM_DEV void st_cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// One CTA owns a tile of TY local rows (TY | B, so the rows are globally consecutive) of
+// one rank column (rid, cid) and walks a chunk of global depths gd, upwards in even chunks
+// and downwards in odd ones, so that two neighbouring chunks read their shared boundary
+// planes at about the same time (the second read comes from L2).  Every step brings the
+// next plane's tile -- its TY rows (one contiguous run of the rank's array) and the y
+// neighbours of its first and last rows (the same or the neighbouring rank) -- into a
+// ring of four shared-memory slots with bulk asynchronous copies (cp.async.bulk, no tensor
+// map, no multicast) completing on one mbarrier per slot, and the x neighbours across the
+// block edges (the last vector of the left rank's row and the first vector of the right
+// rank's, per tile row) with per-thread asynchronous copies (cp.async) into the slot's edge
+// area.  The outputs of depth gd then come from the slots of gd - 1, gd, gd + 1 only (at
+// the periodic x wrap the edge vector is read shifted by one element, as
+// stencil3d_lines_kernel's closed form).  Every plane is read from HBM once, plus two halo
+// rows per TY rows, the x edges and two halo planes per chunk; walking global depth makes
+// the z neighbours across a block edge simply the next plane of the walk.  Same
+// expressions, same order as the other 3D kernels.  A copy that has not landed within two
+// bounded waits raises the plan's device error word; the CTA then stops, after its copies
+// in flight have landed (bounded).
+template <typename S, int TY>
+__global__ void __launch_bounds__(256) stencil3d_march_kernel(const cpx<S> *__restrict__ in, cpx<S> *__restrict__ out,
+                                                              const Geom g, int zsteps, S coef, int *err) {
+    using C = cpx<S>;
+    using O = ops<S>;
+    constexpr bool PAIRS = sizeof(S) == 4;                   // complex64: two elements per 16 bytes
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ uint64_t s_bar[kMarchSlots];
+    const int L = (int)g.L, N = (int)g.n, P = (int)g.p, VEC = (int)g.vec;
+    const int tid = threadIdx.x;
+    const int logL = g.logL, vsh = g.logVEC, vmask = VEC - 1, bl = (int)g.b - 1;
+    // slot: halo row above, TY rows, halo row below; then the edge area [side][row][VEC]
+    const int slotE = (TY + 2) * L + 2 * TY * VEC;
+    C *slots = reinterpret_cast<C *>(smem_raw);
+    // unit of this CTA: (rank column rid * P + cid, depth chunk, row tile), the row tile
+    // fastest so that the CTAs of neighbouring tiles (which share halo rows) and of
+    // neighbouring chunks (which share halo planes) run at the same time
+    const int nchunk = N / zsteps, ntile = L / TY;
+    const int tile = blockIdx.x % ntile;
+    const int zc = (blockIdx.x / ntile) % nchunk;
+    const int col = blockIdx.x / (nchunk * ntile);
+    const int rid = col / P, cid = col % P;
+    const int lr0 = tile * TY;
+    const int gd0 = zc * zsteps;
+    const bool down = (zc & 1) != 0;
+    int ridU, lrU, ridD, lrD;
+    g2l((l2g(lr0, rid, g) - 1 + N) & (N - 1), g, ridU, lrU);
+    g2l((l2g(lr0 + TY - 1, rid, g) + 1) & (N - 1), g, ridD, lrD);
+    const int64_t l3 = (int64_t)L * L * L;
+    // x block edges: the left rank is cid - 1 (cid = 0: P - 1, read shifted by one element),
+    // the right rank cid + 1 (cid = P - 1: 0, shifted the other way)
+    const int64_t dl = cid == 0 ? (int64_t)(P - 1) * l3 : -l3, dr = cid == P - 1 ? -(int64_t)(P - 1) * l3 : l3;
+    const int shl = cid == 0 ? -1 : 0, shr = cid == P - 1 ? 1 : 0;
+    auto row_elem = [&](int rk, int ld, int lr) { return ((((((int64_t)rk << logL) + ld) << logL) + lr) << logL); };
+    const unsigned row_bytes = (unsigned)(L * sizeof(C));
+    // global depth of walk step k (steps 0 and zsteps + 1 are the halo planes)
+    auto step_depth = [&](int k) { return down ? gd0 + zsteps - k : gd0 - 1 + k; };
+    // step k into slot k mod 4 (its (k / 4)-th use: parity (k / 4) & 1)
+    auto issue_bulk = [&](int k) {   // thread 0
+        int did, ld;
+        g2l((step_depth(k) + N) & (N - 1), g, did, ld);
+        const int rk = (did * P + rid) * P + cid;
+        const int rkU = (did * P + ridU) * P + cid, rkD = (did * P + ridD) * P + cid;
+        C *dst = slots + (size_t)(k % kMarchSlots) * slotE;
+        uint64_t *bar = &s_bar[k % kMarchSlots];
+        st_mbar_expect_tx(bar, (unsigned)(TY + 2) * row_bytes);
+        st_bulk_g2s(dst, in + row_elem(rkU, ld, lrU), row_bytes, bar);
+        st_bulk_g2s(dst + L, in + row_elem(rk, ld, lr0), TY * row_bytes, bar);
+        st_bulk_g2s(dst + (size_t)(TY + 1) * L, in + row_elem(rkD, ld, lrD), row_bytes, bar);
+    };
+    // every thread: its share of step k's edge vectors (centre planes only), one group
+    auto issue_edges = [&](int k) {
+        if (k >= 1 && k <= zsteps) {
+            int did, ld;
+            g2l((step_depth(k) + N) & (N - 1), g, did, ld);
+            const int64_t eb = row_elem((did * P + rid) * P + cid, ld, lr0);
+            C *dst = slots + (size_t)(k % kMarchSlots) * slotE + (size_t)(TY + 2) * L;
+            for (int q = tid; q < 2 * TY * VEC; q += blockDim.x) {
+                const int side = q / (TY * VEC), r = (q / VEC) % TY, jj = q & vmask;
+                const int64_t src = eb + ((int64_t)r << logL) + (side ? dr + jj : dl + ((int64_t)bl << vsh) + jj);
+                st_cp_async(dst + q, in + src, (int)sizeof(C));
+            }
+        }
+        st_cp_commit();
+    };
+    auto wait_bounded = [&](int k) {                          // thread 0 only
+        uint64_t *bar = &s_bar[k % kMarchSlots];
+        const unsigned par = (unsigned)((k / kMarchSlots) & 1);
+        if (st_mbar_try_wait(bar, par)) return true;
+        const unsigned long long t0 = st_gtimer_ns();
+        while (!st_mbar_try_wait(bar, par))
+            if (st_gtimer_ns() - t0 > kPlaneWaitNs) return false;
+        return true;
+    };
+    if (tid == 0) {
+        for (int i = 0; i < kMarchSlots; i++) st_mbar_init(&s_bar[i], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const int nsteps = zsteps + 2;                            // zsteps >= 16: nsteps > 4
+    int issued = 0;                                           // steps issued (uniform count)
+    for (; issued < kMarchSlots; issued++) {
+        if (tid == 0) issue_bulk(issued);
+        issue_edges(issued);
+    }
+    bool lost = false;                                        // block-uniform
+    int waited = 0;                                           // steps whose bulk copies have landed
+    auto wait_step = [&](int k) {
+        bool ok = true;
+        if (tid == 0) {
+            ok = wait_bounded(k) || wait_bounded(k);          // two bounded waits, as the FFT passes
+            if (!ok && err) atomicExch(err, 1);
+        }
+        lost = __syncthreads_or(!ok) != 0;
+        if (!lost) waited = k + 1;
+    };
+    wait_step(0);
+    if (!lost) wait_step(1);
+    const int per_plane = TY * L;
+    for (int z = 0; z < zsteps && !lost; z++) {
+        // edges of step z + 1: groups issued so far = z + 4, the last two may be pending
+        st_cp_wait<2>();
+        wait_step(z + 2);                                     // also publishes the edge copies
+        if (lost) break;
+        const C *p0 = slots + (size_t)(z % kMarchSlots) * slotE;
+        const C *pc = slots + (size_t)((z + 1) % kMarchSlots) * slotE;
+        const C *p2 = slots + (size_t)((z + 2) % kMarchSlots) * slotE;
+        const C *pm = down ? p2 : p0;                         // depth gd - 1
+        const C *pp = down ? p0 : p2;                         // depth gd + 1
+        const C *eL = pc + (size_t)(TY + 2) * L, *eR = eL + TY * VEC;
+        int did, ld;
+        g2l(step_depth(z + 1), g, did, ld);
+        C *orow = out + row_elem((did * P + rid) * P + cid, ld, lr0);
+        auto lap = [&](const C &up, const C &dn, const C &lf, const C &rt, const C &fr, const C &bk, const C &cc) {
+            S rx = O::add((S)0, up.x), ry = O::add((S)0, up.y);
+            rx = O::add(rx, dn.x);
+            ry = O::add(ry, dn.y);
+            rx = O::add(rx, lf.x);
+            ry = O::add(ry, lf.y);
+            rx = O::add(rx, rt.x);
+            ry = O::add(ry, rt.y);
+            rx = O::add(rx, fr.x);
+            ry = O::add(ry, fr.y);
+            rx = O::add(rx, bk.x);
+            ry = O::add(ry, bk.y);
+            rx = O::fmaop((S)(-6), cc.x, rx);
+            ry = O::fmaop((S)(-6), cc.y, ry);
+            return C{O::mul(rx, coef), O::mul(ry, coef)};
+        };
+        if (PAIRS && VEC >= 2) {
+            // complex64, two adjacent elements per thread (same row, same vector j): every
+            // slot access and the store are 16-byte vectors, except across a block edge
+            using C2 = float4;
+            auto ld2 = [](const C *p, C &a, C &b) {
+                const C2 q = *reinterpret_cast<const C2 *>(p);
+                a = C{(S)q.x, (S)q.y};
+                b = C{(S)q.z, (S)q.w};
+            };
+            for (int h = tid; h < per_plane / 2; h += blockDim.x) {
+                const int e = 2 * h;
+                const int r = e >> logL, pos = e & (L - 1);
+                const int c = (r + 1) * L + pos;
+                const int j = pos >> vsh, jj = pos & vmask;
+                C lf0, lf1, rt0, rt1, up0, up1, dn0, dn1, fr0, fr1, bk0, bk1, c0, c1;
+                if (j > 0) {
+                    ld2(pc + c - VEC, lf0, lf1);
+                } else {
+                    lf0 = eL[r * VEC + ((jj + shl) & vmask)];
+                    lf1 = eL[r * VEC + ((jj + 1 + shl) & vmask)];
+                }
+                if (j < bl) {
+                    ld2(pc + c + VEC, rt0, rt1);
+                } else {
+                    rt0 = eR[r * VEC + ((jj + shr) & vmask)];
+                    rt1 = eR[r * VEC + ((jj + 1 + shr) & vmask)];
+                }
+                ld2(pc + c - L, up0, up1);
+                ld2(pc + c + L, dn0, dn1);
+                ld2(pm + c, fr0, fr1);
+                ld2(pp + c, bk0, bk1);
+                ld2(pc + c, c0, c1);
+                const C o0 = lap(up0, dn0, lf0, rt0, fr0, bk0, c0), o1 = lap(up1, dn1, lf1, rt1, fr1, bk1, c1);
+                *reinterpret_cast<C2 *>(orow + e) = make_float4((float)o0.x, (float)o0.y, (float)o1.x, (float)o1.y);
+            }
+        } else {
+            for (int e = tid; e < per_plane; e += blockDim.x) {
+                const int r = e >> logL, pos = e & (L - 1);      // tile row, packed position
+                const int c = (r + 1) * L + pos;                   // centre's slot element
+                const int j = pos >> vsh, jj = pos & vmask;
+                const C lf = j > 0 ? pc[c - VEC] : eL[r * VEC + ((jj + shl) & vmask)];
+                const C rt = j < bl ? pc[c + VEC] : eR[r * VEC + ((jj + shr) & vmask)];
+                orow[e] = lap(pc[c - L], pc[c + L], lf, rt, pm[c], pp[c], pc[c]);
+            }
+        }
+        __syncthreads();                                       // the slot of step z is free
+        if (issued < nsteps) {
+            if (tid == 0) issue_bulk(issued);
+            issue_edges(issued);
+            issued++;
+        } else {
+            st_cp_commit();                                    // keep the group count uniform
+        }
+    }
+    st_cp_wait<0>();
+    // after a wait gave up: let the bulk copies still in flight land (bounded) before exiting
+    if (lost && tid == 0)
+        for (int k = waited; k < issued; k++) wait_bounded(k);
+}
+
+// The plane-tile 3D Laplacian where its shape applies (complex fields; tiles of
+// TY = min(8 complex64 / 4 complex128, B) rows dividing B and L; the four slots within
+// 200 KB of shared memory); cudaErrorNotSupported otherwise, and the caller uses
+// stencil3d_lines_kernel.
+template <typename S, int TY>
+static cudaError_t launch_march_ty(const zm_plan_s *p, const S *in, S *out, S coef, cudaStream_t st) {
+    const Geom &g = p->g;
+    const size_t smem = (size_t)kMarchSlots * ((TY + 2) * g.L + 2 * TY * g.vec) * sizeof(cpx<S>);
+    if (smem > 200 * 1024) return cudaErrorNotSupported;
+    auto kern = stencil3d_march_kernel<S, TY>;
+    static int attr_done[64];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorNotSupported;
+    if (!attr_done[dev]) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (e != cudaSuccess) return e;
+        attr_done[dev] = 1;
+    }
+    int per_sm = 0, sms = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorNotSupported;
+    const int64_t cols = g.p * g.p, tiles = g.L / TY;
+    // depth chunks: at least four waves of resident CTAs (a short tail), each chunk walking
+    // >= 16 depths; its two halo planes are read at the same time by the neighbouring
+    // chunk's CTA (next in launch order, walking the other way), mostly from L2
+    int64_t chunks = 1;
+    while (cols * tiles * chunks < 4 * (int64_t)per_sm * sms && g.n / (chunks * 2) >= 16) chunks *= 2;
+    const int zsteps = (int)(g.n / chunks);
+    kern<<<(unsigned)(cols * tiles * chunks), 256, smem, st>>>(reinterpret_cast<const cpx<S> *>(in),
+                                                               reinterpret_cast<cpx<S> *>(out), g, zsteps, coef,
+                                                               p->dev_err);
+    return cudaGetLastError();
+}
+template <typename S>
+static cudaError_t launch_march(const zm_plan_s *p, const S *in, S *out, S coef, cudaStream_t st) {
+    const Geom &g = p->g;
+    const int64_t tymax = sizeof(S) == 4 ? 8 : 4;
+    const int64_t ty = g.b < tymax ? g.b : tymax;
+    if (g.dim != 3 || g.L % ty || g.b % ty || g.n < 16) return cudaErrorNotSupported;
+    if (ty == 8) return launch_march_ty<S, 8>(p, in, out, coef, st);
+    if (ty == 4) return launch_march_ty<S, 4>(p, in, out, coef, st);
+    if (ty == 2) return launch_march_ty<S, 2>(p, in, out, coef, st);
+    return cudaErrorNotSupported;
+}
+
 template <typename S, int NC>
 static cudaError_t launch_s(const zm_plan_s *p, int op, const void *in, void *out, void *out2, void *out3,
                             double coef, double coef2, cudaStream_t st) {
@@ -532,6 +833,11 @@ static cudaError_t launch_s(const zm_plan_s *p, int op, const void *in, void *ou
             stencil_kernel<S, NC, ST_ALL, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
     } else {
         if (op != ST_LAPLACE) return cudaErrorInvalidValue;
+        if (NC == 2) {
+            const cudaError_t em = launch_march<S>(p, i, o, c, st);
+            if (em == cudaSuccess) count_launch();
+            if (em != cudaErrorNotSupported) return em;   // launched (or failed): done
+        }
         // vectors of one line per thread: 4 for one complex128 per vector, else 2
         constexpr int RX = K == 1 ? 4 : 2;
         const int64_t vline = p->g.L / K;       // vectors per line

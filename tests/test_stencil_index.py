@@ -125,3 +125,87 @@ def test_laplace3d_global_line_order_is_a_permutation(n, b, p):
     rank = (did * p + rid) * p + cid
     line = (((rank << logL) + ld) << logL) + lr
     assert np.array_equal(np.sort(line), np.arange(p ** 3 * L * L))
+
+
+def march_neighbours(n, b, p, ty, zsteps):
+    """Element index of each neighbour of each element as stencil3d_march_kernel reads it:
+    a CTA owns local rows lr0 .. lr0 + ty - 1 of rank column (rid, cid) and walks a chunk
+    of zsteps global depths, upwards in even chunks and downwards in odd ones; walk step k
+    fills slot k mod 4 with rows [halo above, ty rows, halo below] of the rank of its depth
+    (halos through the block-cyclic row maps) and, for centre planes, an edge area with the
+    last vector of the left rank's row and the first vector of the right rank's row per
+    tile row; y / z neighbours come from the slots, x neighbours from the slot row or,
+    across a block edge, from the edge area (shifted by one element at the periodic wrap)."""
+    L = n // p
+    vec = L // b
+    logB, logP, logL, logVEC = lg(b), lg(p), lg(L), lg(vec)
+
+    def l2g(li, i):
+        return ((li >> logB) << (logB + logP)) + (i << logB) + (li & (b - 1))
+
+    def g2l(gi):
+        return (gi >> logB) & (p - 1), ((gi >> (logB + logP)) << logB) + (gi & (b - 1))
+
+    def row_elem(rk, ld, lr):
+        return ((rk * L + ld) * L + lr) * L
+
+    total = L ** 3 * p ** 3
+    out = {k: np.full(total, -1, dtype=np.int64) for k in ("up", "dn", "lf", "rt", "fr", "bk")}
+    l3 = L ** 3
+    pos = np.arange(L)
+    j, jj = pos >> logVEC, pos & (vec - 1)
+    for rid in range(p):
+        for cid in range(p):
+            dl = (p - 1) * l3 if cid == 0 else -l3
+            dr = -(p - 1) * l3 if cid == p - 1 else l3
+            shl = -1 if cid == 0 else 0
+            shr = 1 if cid == p - 1 else 0
+            for lr0 in range(0, L, ty):
+                ridU, lrU = g2l((l2g(lr0, rid) - 1 + n) % n)
+                ridD, lrD = g2l((l2g(lr0 + ty - 1, rid) + 1) % n)
+                for zc in range(n // zsteps):
+                    gd0, down = zc * zsteps, zc % 2 == 1
+
+                    def depth(k):
+                        return gd0 + zsteps - k if down else gd0 - 1 + k
+
+                    def slot(k):   # (rows, left edge vectors, right edge vectors)
+                        did, ld = g2l(depth(k) % n)
+                        rk = (did * p + rid) * p + cid
+                        rows = [row_elem((did * p + ridU) * p + cid, ld, lrU)]
+                        rows += [row_elem(rk, ld, lr0 + r) for r in range(ty)]
+                        rows += [row_elem((did * p + ridD) * p + cid, ld, lrD)]
+                        eb = row_elem(rk, ld, lr0)
+                        el = [eb + r * L + dl + (b - 1) * vec + np.arange(vec) for r in range(ty)]
+                        er = [eb + r * L + dr + np.arange(vec) for r in range(ty)]
+                        return rows, el, er
+                    for z in range(zsteps):
+                        s0, sc, s2 = slot(z), slot(z + 1), slot(z + 2)
+                        sm, sp = (s2, s0) if down else (s0, s2)
+                        for r in range(ty):
+                            ec = sc[0][r + 1]
+                            e = ec + pos
+                            out["up"][e] = sc[0][r] + pos
+                            out["dn"][e] = sc[0][r + 2] + pos
+                            out["fr"][e] = sm[0][r + 1] + pos
+                            out["bk"][e] = sp[0][r + 1] + pos
+                            out["lf"][e] = np.where(j > 0, ec + pos - vec, sc[1][r][(jj + shl) & (vec - 1)])
+                            out["rt"][e] = np.where(j < b - 1, ec + pos + vec, sc[2][r][(jj + shr) & (vec - 1)])
+    return out
+
+
+@pytest.mark.parametrize("n,b,p", [(16, 4, 2), (32, 4, 2), (64, 4, 4), (64, 8, 2), (64, 16, 2), (32, 8, 1)])
+def test_laplace3d_plane_tiles_match_layout(n, b, p):
+    """The plane-tile kernel's neighbour addressing equals the true neighbours for every
+    element (tile heights as the launcher picks them: min(8, B) for complex64 and
+    min(4, B) for complex128; one chunk of all depths, and chunks of 8 walked in
+    alternating directions)."""
+    ref = true_neighbours(n, b, p)
+    for ty in sorted({min(8, b), min(4, b)}):
+        if ty < 2 or (n // p) % ty:
+            continue
+        for zsteps in sorted({n, 8}):
+            got = march_neighbours(n, b, p, ty, zsteps)
+            for nm in ref:
+                assert (got[nm] >= 0).all(), (nm, ty, zsteps)
+                assert np.array_equal(got[nm], ref[nm]), (nm, ty, zsteps)
