@@ -126,9 +126,6 @@ ZM_DEV int field_of_tile(const BatchField *fields, int nfields, int64_t tile) {
     return lo;
 }
 
-// signed frequency
-ZM_DEV double sfreq(int64_t k, const Geom &g) { return (double)(k >= (g.n >> 1) ? k - g.n : k); }
-
 // global (row, col) -> element of the real layout (inverse of real_gidx, 2D)
 ZM_DEV int64_t real_elem(int64_t gr, int64_t gc, const Geom &g) {
     const int64_t rid = (gr >> g.logB) & (g.p - 1);
@@ -141,9 +138,11 @@ ZM_DEV int64_t real_elem(int64_t gr, int64_t gc, const Geom &g) {
 // Both sub-transforms of a tile: compile-time-sized stages (LMC = log2 M) for the
 // complex64 tiles with VEC = 4 (the layout the B autotuner picks for the batch sizes, B =
 // N / 8 at P = 2), or the runtime-sized stages (LMC = 0) for every other shape.
+// (LMC > 0: the column sub-transform only; the row stage runs fused with the
+// vector-side sweep, tile_load_rows_v4 / tile_rows_store_v4)
 template <typename T, int EPT, bool INV, int LM, typename SW>
 __device__ __noinline__ void tile_transform_v4(cpx<T> *s, int tid, const tw<T> *twN) {
-    tile_transform_ct<T, EPT, INV, 2, LM, kBatchThreads, SW>(s, tid, twN);
+    tile_transform_ct<T, EPT, INV, 2, LM, kBatchThreads, SW, false>(s, tid, twN);
 }
 template <typename T, int EPT, bool INV, int LMC, typename SW>
 ZM_DEV void batch_tile_transform(cpx<T> *s, const BatchField &f, int nthr, int tid, const tw<T> *twN) {
@@ -163,8 +162,17 @@ __device__ __noinline__ void batch_tile(int op, bool scale, double a, const Batc
     const Geom &g = sf.g;
     const tw<T> *twN = reinterpret_cast<const tw<T> *>(sf.twN);
     const bool xpass = op == BOP_X_FWD || op == BOP_X_INV;
+    // vector-side sweeps: plain, or with the VEC = 4 row stage fused in (LMC > 0)
+    auto load_vec = [&]() {
+        if constexpr (LMC > 0) tile_load_rows_v4<EPT, LMC, kBatchThreads, SW>(c, g, s, in, tid);
+        else tile_load_vec<EPT, SW>(c, g, s, in, nthr, tid);
+    };
+    auto store_vec = [&](bool scl, T sc) {
+        if constexpr (LMC > 0) tile_rows_store_v4<EPT, LMC, kBatchThreads, SW>(c, g, s, out, scl, sc, (T)0, twN, tid);
+        else tile_store_vec<EPT, SW>(c, g, s, out, scl, sc, (T)0, nthr, tid);
+    };
     if (op == BOP_X_FWD || op == BOP_Y_FWD) {
-        tile_load_vec<EPT, SW>(c, g, s, in, nthr, tid);
+        load_vec();
         __syncthreads();
         batch_tile_transform<T, EPT, false, LMC, SW>(s, sf, nthr, tid, twN);
         tile_store_freq<EPT, SW>(c, g, s, out, false, (T)1, (T)0, nthr, tid);
@@ -174,32 +182,35 @@ __device__ __noinline__ void batch_tile(int op, bool scale, double a, const Batc
         batch_tile_transform<T, EPT, true, LMC, SW>(s, sf, nthr, tid, twN);
         const bool scl = scale && xpass;
         const T sc = (T)(1.0 / ((double)g.n * (double)g.n));
-        tile_store_vec<EPT, SW>(c, g, s, out, scl, sc, (T)0, nthr, tid);
+        store_vec(scl, sc);
     } else {   // BOP_Y_POISSON
-        tile_load_vec<EPT, SW>(c, g, s, in, nthr, tid);
+        load_vec();
         __syncthreads();
         batch_tile_transform<T, EPT, false, LMC, SW>(s, sf, nthr, tid, twN);
         // slot (t, k1, k2) holds the frequency the y pass would store at rank
         // (rid = k2 / VP, cid), local row p, column pos = k1 VP + k2 % VP
-        // (reciprocal_to_global, utils.h:265-268)
+        // (reciprocal_to_global, utils.h:265-268): along the transform that is
+        // d_ct(rid L + d_lp(pos)) = d_ct(k2 M + k1) = k1 VEC + k2 = r, the slot position
+        // itself; along the lines d_ct(cid L + d_lp(p)) of line l0 + t.  The factor
+        // -1 / (a^2 |k|^2) in the working precision (|k|^2 an exact integer).
         const int tot = sf.T << g.logN;
-        const double a2 = a * a;
+        const int nh = (int)(g.n >> 1);
+        const T a2 = (T)(a * a);
         for (int e = tid; e < tot; e += nthr) {
             const int t = e >> g.logN, r = e & (int)(g.n - 1);
-            const int k1 = r >> g.logVEC, k2 = r & (int)(g.vec - 1);
-            const int64_t rid = k2 >> g.logVP;
-            const int64_t pos = ((int64_t)k1 << g.logVP) + (k2 & (int)(g.vp - 1));
             const int64_t l = l0 + t, cid = l >> g.logL, p = l & (g.L - 1);
-            const double sa = sfreq(d_ct(cid * g.L + d_lp(p, g), g), g);
-            const double sb = sfreq(d_ct(rid * g.L + d_lp(pos, g), g), g);
-            const double ksq = sa * sa + sb * sb;
-            const double fac = ksq == 0.0 ? 0.0 : -1.0 / (a2 * ksq);
+            const int ka = (int)d_ct(cid * g.L + d_lp(p, g), g);
+            const int sa = ka >= nh ? ka - (int)g.n : ka, sb = r >= nh ? r - (int)g.n : r;
+            const int ksq = sa * sa + sb * sb;
+            T fac;
+            if constexpr (sizeof(T) == 4) fac = ksq == 0 ? 0.f : -__frcp_rn(a2 * (float)ksq);
+            else fac = ksq == 0 ? 0.0 : -1.0 / (a2 * (double)ksq);
             const cpx<T> v = s[SW::f(e)];
-            s[SW::f(e)] = {(T)(v.x * fac), (T)(v.y * fac)};
+            s[SW::f(e)] = {v.x * fac, v.y * fac};
         }
         __syncthreads();
         batch_tile_transform<T, EPT, true, LMC, SW>(s, sf, nthr, tid, twN);
-        tile_store_vec<EPT, SW>(c, g, s, out, false, (T)1, (T)0, nthr, tid);
+        store_vec(false, (T)1);
     }
 }
 

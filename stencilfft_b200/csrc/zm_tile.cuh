@@ -208,15 +208,16 @@ ZM_DEV void run_subfft_ct(cpx<T> *s, int tid, const tw<T> *twN) {
     }
 }
 
-template <typename T, int EPT, bool INV, int LV, int LM, int NT, typename SW = SwzNone>
+// ROWS = false leaves out the row sub-transform (done by the fused row sweeps below).
+template <typename T, int EPT, bool INV, int LV, int LM, int NT, typename SW = SwzNone, bool ROWS = true>
 ZM_DEV void tile_transform_ct(cpx<T> *s, int tid, const tw<T> *twN) {
     constexpr int RL = EPT >= 16 ? 4 : 3;   // radix_schedule(n, EPT): largest radix EPT
     if constexpr (!INV) {
-        run_subfft_ct<0, 1, EPT, false, -1, false, T, LV, LM, LV, NT, RL, SW>(s, tid, twN);
+        if constexpr (ROWS) run_subfft_ct<0, 1, EPT, false, -1, false, T, LV, LM, LV, NT, RL, SW>(s, tid, twN);
         run_subfft_ct<0, 1, EPT, true, -1, true, T, LV, LM, LM, NT, RL, SW>(s, tid, twN);
     } else {
         run_subfft_ct<0, 1, EPT, true, 1, false, T, LV, LM, LM, NT, RL, SW>(s, tid, twN);
-        run_subfft_ct<0, 1, EPT, false, 1, true, T, LV, LM, LV, NT, RL, SW>(s, tid, twN);
+        if constexpr (ROWS) run_subfft_ct<0, 1, EPT, false, 1, true, T, LV, LM, LV, NT, RL, SW>(s, tid, twN);
     }
 }
 
@@ -335,6 +336,63 @@ ZM_DEV void tile_store_vec(const Tile &c, const Geom &g, const cpx<T> *s, cpx<T>
         cpx<T> v = s[SW::f(e)];
         if (scl) v = {sr * v.x - si * v.y, sr * v.y + si * v.x};
         out[c.abase[t] + ch * c.a_chunk + pos] = v;
+    }
+}
+
+// ------------------------------------ complex64 VEC = 4 tiles: row stage fused with the sweep
+// With VEC = 4 the row sub-transform is one radix-4 stage over rows of 4 consecutive
+// vector-side positions (n1 VEC .. n1 VEC + 3, contiguous when the vector side is, a_pos
+// = 1, and 32-byte aligned).  Thread tid takes rows rho = tid + q NT (q < EPT / 4), the
+// rows stockham_stage_ct gives it, and the same arithmetic in the same order:
+//   forward: two 16-byte loads per row, the radix-4 DFT in registers, the four outputs
+//            to their slots (the stage's output order is natural: one stage, NS = 1);
+//   inverse: the row's four slots, the conjugate inter-step twiddles w_N^{-n1 k2}
+//            (k2 = 0 .. 3), the radix-4 DFT, the optional scale of tile_store_vec, two
+//            16-byte stores.
+// This drops one shared-memory round trip and its two barriers per tile.
+template <int EPT, int LM, int NT, typename SW>
+ZM_DEV void tile_load_rows_v4(const Tile &c, const Geom &g, cpx<float> *s, const cpx<float> *in, int tid) {
+    constexpr int RPT = EPT / 4, M = 1 << LM;
+    float4 v[RPT][2];
+#pragma unroll
+    for (int q = 0; q < RPT; q++) {
+        const int rho = tid + q * NT;
+        const int t = rho >> LM, r = (rho & (M - 1)) << 2;
+        const int ch = r >> g.logL, pos = r & (int)(g.L - 1);
+        const float4 *p = reinterpret_cast<const float4 *>(in + c.abase[t] + ch * c.a_chunk + pos);
+        v[q][0] = __ldg(p);
+        v[q][1] = __ldg(p + 1);
+    }
+#pragma unroll
+    for (int q = 0; q < RPT; q++) {
+        cpx<float> x[4] = {{v[q][0].x, v[q][0].y}, {v[q][0].z, v[q][0].w}, {v[q][1].x, v[q][1].y},
+                           {v[q][1].z, v[q][1].w}};
+        dft<4, -1, float>(x);
+        const int rho = tid + q * NT;
+#pragma unroll
+        for (int k = 0; k < 4; k++) s[SW::f(rho * 4 + k)] = x[k];
+    }
+}
+template <int EPT, int LM, int NT, typename SW>
+ZM_DEV void tile_rows_store_v4(const Tile &c, const Geom &g, const cpx<float> *s, cpx<float> *out, bool scl,
+                               float sr, float si, const tw<float> *twN, int tid) {
+    constexpr int RPT = EPT / 4, M = 1 << LM;
+#pragma unroll
+    for (int q = 0; q < RPT; q++) {
+        const int rho = tid + q * NT;
+        const int n1 = rho & (M - 1);
+        cpx<float> x[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) x[k] = twmul<true>(s[SW::f(rho * 4 + k)], ldtw(twN, (int64_t)k * n1));
+        dft<4, 1, float>(x);
+        if (scl)
+#pragma unroll
+            for (int k = 0; k < 4; k++) x[k] = {sr * x[k].x - si * x[k].y, sr * x[k].y + si * x[k].x};
+        const int t = rho >> LM, r = n1 << 2;
+        const int ch = r >> g.logL, pos = r & (int)(g.L - 1);
+        float4 *p = reinterpret_cast<float4 *>(out + c.abase[t] + ch * c.a_chunk + pos);
+        p[0] = make_float4(x[0].x, x[0].y, x[1].x, x[1].y);
+        p[1] = make_float4(x[2].x, x[2].y, x[3].x, x[3].y);
     }
 }
 

@@ -15,7 +15,10 @@ from helpers import TOL, relerr, to_host
 
 pytestmark = pytest.mark.gpu
 
-MIXED = [(64, 4, 2), (128, 8, 2), (256, 16, 2), (128, 2, 4), (512, 32, 4), (64, 16, 2), (256, 1, 2)]
+# (the VEC = 4 complex64 tiles, whose row stage runs fused with the vector-side sweeps, at
+# M = 16, 64, 128, 256, 512: (64, 8, 2), (256, 32, 2), (512, 32, 4), (1024, 128, 2), (2048, 256, 2))
+MIXED = [(64, 4, 2), (128, 8, 2), (256, 16, 2), (128, 2, 4), (512, 32, 4), (64, 16, 2), (256, 1, 2),
+         (64, 8, 2), (256, 32, 2), (1024, 128, 2), (2048, 256, 2)]
 
 
 def _batch(fields, dt):
