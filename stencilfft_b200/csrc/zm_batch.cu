@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batch_kernel(const BatchPara
     cpx<T> *s = reinterpret_cast<cpx<T> *>(smem_raw);
     __shared__ int64_t s_abase[64], s_fbase[64];
     __shared__ BatchField sf;
-    __shared__ int s_ok;
+    __shared__ int s_ok, s_f;
     const int tid = threadIdx.x, nthr = blockDim.x;
 
     for (int st = 0; st < bp.nsteps; st++) {
@@ -229,16 +229,25 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batch_kernel(const BatchPara
         if (S.op == BOP_NOP) continue;
 
         if (S.op == BOP_RESIDUAL || S.op == BOP_FILL) {
-            // element-wise steps: field by field, grid-stride inside each field
-            const int64_t stride = (int64_t)gridDim.x * nthr;
-            for (int f = 0; f < bp.nfields; f++) {
-                const BatchField &F = bp.fields[f];
-                const Geom g = F.g;
-                const int64_t total = g.n * g.n;
-                cpx<T> *out = reinterpret_cast<cpx<T> *>(S.out) + F.off;
+            // element-wise steps over the pass steps' tiles: tile `tile` of field f covers
+            // elements [(tile - tile0) * TP, + TP) of the field's array (N^2 / TP tiles of a
+            // field of N^2 elements), so every CTA has work whatever the field sizes
+            constexpr int TP = kBatchThreads * EPT;
+            for (int64_t tile = blockIdx.x; tile < bp.tiles; tile += gridDim.x) {
+                __syncthreads();   // the previous tile is done with sf
+                if (tid == 0) {
+                    s_f = field_of_tile(bp.fields, bp.nfields, tile);
+                    sf = bp.fields[s_f];
+                }
+                __syncthreads();
+                const int f = s_f;
+                const Geom g = sf.g;
+                const int64_t e0 = (tile - sf.tile0) * TP;
+                cpx<T> *out = reinterpret_cast<cpx<T> *>(S.out) + sf.off;
                 if (S.op == BOP_FILL) {
                     const uint64_t seed = S.seed + (uint64_t)f;
-                    for (int64_t e = (int64_t)blockIdx.x * nthr + tid; e < total; e += stride) {
+                    for (int i = tid; i < TP; i += nthr) {
+                        const int64_t e = e0 + i;
                         const uint64_t gi = (uint64_t)real_gidx(e, g);
                         double re, im;
                         if (S.kind == 0) {
@@ -250,64 +259,65 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batch_kernel(const BatchPara
                         }
                         out[e] = {(T)re, (T)im};
                     }
-                } else {
-                    const cpx<T> *in = reinterpret_cast<const cpx<T> *>(S.in) + F.off;
-                    const cpx<T> *rhs = reinterpret_cast<const cpx<T> *>(S.aux) + F.off;
-                    const T inv_h2 = (T)((double)g.n * S.a * (double)g.n * S.a);
-                    const int64_t m = g.n - 1;
-                    auto resid = [&](const cpx<T> &up, const cpx<T> &dn, const cpx<T> &lf, const cpx<T> &rt,
-                                     const cpx<T> &c, const cpx<T> &r) -> cpx<T> {
-                        const T lx = up.x + dn.x + lf.x + rt.x - (T)4 * c.x;
-                        const T ly = up.y + dn.y + lf.y + rt.y - (T)4 * c.y;
-                        return {lx * inv_h2 - r.x, ly * inv_h2 - r.y};
+                    continue;
+                }
+                const cpx<T> *in = reinterpret_cast<const cpx<T> *>(S.in) + sf.off;
+                const cpx<T> *rhs = reinterpret_cast<const cpx<T> *>(S.aux) + sf.off;
+                const T inv_h2 = (T)((double)g.n * S.a * (double)g.n * S.a);
+                const int64_t m = g.n - 1;
+                auto resid = [&](const cpx<T> &up, const cpx<T> &dn, const cpx<T> &lf, const cpx<T> &rt,
+                                 const cpx<T> &c, const cpx<T> &r) -> cpx<T> {
+                    const T lx = up.x + dn.x + lf.x + rt.x - (T)4 * c.x;
+                    const T ly = up.y + dn.y + lf.y + rt.y - (T)4 * c.y;
+                    return {lx * inv_h2 - r.x, ly * inv_h2 - r.y};
+                };
+                if constexpr (sizeof(T) == 4) {
+                    // Pairs (e, e + 1), e even: the two share rank and row (L is even), so
+                    // their up / down neighbours are again two adjacent elements, and so
+                    // are left / right except at a block edge.  Adjacent 16-byte-aligned
+                    // pairs move as one 16-byte access, anything else element by element.
+                    auto ld2 = [](const cpx<T> *p0, const cpx<T> *p1, cpx<T> &v0, cpx<T> &v1) {
+                        if (p1 == p0 + 1 && ((uintptr_t)p0 & 15) == 0) {
+                            const float4 q = __ldg(reinterpret_cast<const float4 *>(p0));
+                            v0 = {q.x, q.y};
+                            v1 = {q.z, q.w};
+                        } else {
+                            v0 = ldg(p0);
+                            v1 = ldg(p1);
+                        }
                     };
-                    if constexpr (sizeof(T) == 4) {
-                        // Pairs (e, e + 1), e even: the two share rank and row (L is even), so
-                        // their up / down neighbours are again two adjacent elements, and so
-                        // are left / right except at a block edge.  Adjacent 16-byte-aligned
-                        // pairs move as one 16-byte access, anything else element by element.
-                        auto ld2 = [](const cpx<T> *p0, const cpx<T> *p1, cpx<T> &v0, cpx<T> &v1) {
-                            if (p1 == p0 + 1 && ((uintptr_t)p0 & 15) == 0) {
-                                const float4 q = __ldg(reinterpret_cast<const float4 *>(p0));
-                                v0 = {q.x, q.y};
-                                v1 = {q.z, q.w};
-                            } else {
-                                v0 = ldg(p0);
-                                v1 = ldg(p1);
-                            }
-                        };
-                        for (int64_t h = (int64_t)blockIdx.x * nthr + tid; h < (total >> 1); h += stride) {
-                            const int64_t e = 2 * h;
-                            const int64_t gi0 = real_gidx(e, g), gc1 = real_gidx(e + 1, g) & m;
-                            const int64_t gr = gi0 >> g.logN, gc0 = gi0 & m;
-                            const int64_t au = real_elem((gr - 1) & m, gc0, g), ad = real_elem((gr + 1) & m, gc0, g);
-                            cpx<T> up0, up1, dn0, dn1, lf0, lf1, rt0, rt1, c0, c1, r0, r1;
-                            ld2(in + au, in + au + 1, up0, up1);
-                            ld2(in + ad, in + ad + 1, dn0, dn1);
-                            ld2(in + real_elem(gr, (gc0 - 1) & m, g), in + real_elem(gr, (gc1 - 1) & m, g), lf0, lf1);
-                            ld2(in + real_elem(gr, (gc0 + 1) & m, g), in + real_elem(gr, (gc1 + 1) & m, g), rt0, rt1);
-                            ld2(in + e, in + e + 1, c0, c1);
-                            ld2(rhs + e, rhs + e + 1, r0, r1);
-                            const cpx<T> o0 = resid(up0, dn0, lf0, rt0, c0, r0);
-                            const cpx<T> o1 = resid(up1, dn1, lf1, rt1, c1, r1);
-                            cpx<T> *po = out + e;
-                            if (((uintptr_t)po & 15) == 0) {
-                                *reinterpret_cast<float4 *>(po) = make_float4(o0.x, o0.y, o1.x, o1.y);
-                            } else {
-                                po[0] = o0;
-                                po[1] = o1;
-                            }
+                    for (int i = tid; i < TP / 2; i += nthr) {
+                        const int64_t e = e0 + 2 * i;
+                        const int64_t gi0 = real_gidx(e, g), gc1 = real_gidx(e + 1, g) & m;
+                        const int64_t gr = gi0 >> g.logN, gc0 = gi0 & m;
+                        const int64_t au = real_elem((gr - 1) & m, gc0, g), ad = real_elem((gr + 1) & m, gc0, g);
+                        cpx<T> up0, up1, dn0, dn1, lf0, lf1, rt0, rt1, c0, c1, r0, r1;
+                        ld2(in + au, in + au + 1, up0, up1);
+                        ld2(in + ad, in + ad + 1, dn0, dn1);
+                        ld2(in + real_elem(gr, (gc0 - 1) & m, g), in + real_elem(gr, (gc1 - 1) & m, g), lf0, lf1);
+                        ld2(in + real_elem(gr, (gc0 + 1) & m, g), in + real_elem(gr, (gc1 + 1) & m, g), rt0, rt1);
+                        ld2(in + e, in + e + 1, c0, c1);
+                        ld2(rhs + e, rhs + e + 1, r0, r1);
+                        const cpx<T> o0 = resid(up0, dn0, lf0, rt0, c0, r0);
+                        const cpx<T> o1 = resid(up1, dn1, lf1, rt1, c1, r1);
+                        cpx<T> *po = out + e;
+                        if (((uintptr_t)po & 15) == 0) {
+                            *reinterpret_cast<float4 *>(po) = make_float4(o0.x, o0.y, o1.x, o1.y);
+                        } else {
+                            po[0] = o0;
+                            po[1] = o1;
                         }
-                    } else {
-                        for (int64_t e = (int64_t)blockIdx.x * nthr + tid; e < total; e += stride) {
-                            const int64_t gi = real_gidx(e, g);
-                            const int64_t gr = gi >> g.logN, gc = gi & m;
-                            const cpx<T> up = ldg(in + real_elem((gr - 1) & m, gc, g));
-                            const cpx<T> dn = ldg(in + real_elem((gr + 1) & m, gc, g));
-                            const cpx<T> lf = ldg(in + real_elem(gr, (gc - 1) & m, g));
-                            const cpx<T> rt = ldg(in + real_elem(gr, (gc + 1) & m, g));
-                            out[e] = resid(up, dn, lf, rt, ldg(in + e), ldg(rhs + e));
-                        }
+                    }
+                } else {
+                    for (int i = tid; i < TP; i += nthr) {
+                        const int64_t e = e0 + i;
+                        const int64_t gi = real_gidx(e, g);
+                        const int64_t gr = gi >> g.logN, gc = gi & m;
+                        const cpx<T> up = ldg(in + real_elem((gr - 1) & m, gc, g));
+                        const cpx<T> dn = ldg(in + real_elem((gr + 1) & m, gc, g));
+                        const cpx<T> lf = ldg(in + real_elem(gr, (gc - 1) & m, g));
+                        const cpx<T> rt = ldg(in + real_elem(gr, (gc + 1) & m, g));
+                        out[e] = resid(up, dn, lf, rt, ldg(in + e), ldg(rhs + e));
                     }
                 }
             }
