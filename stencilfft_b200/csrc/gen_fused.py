@@ -3,7 +3,9 @@ dispatch tables.  Each (log2 VEC, log2 M) pair lists variants (cluster size CL, 
 per tile TL, threads NT[, "p" = persistent forward pass with bulk-copy prefetch]); the
 plan's `variant` picks one; "k3" marks the three-stage 512-thread pass of zm_fft3.cuh
 for complex64 lines of 2^14 points ("k3p": its persistent form with asynchronous copies
-of the next line; "k3c": the forward y pass on buddy-line CTA pairs).  Variant 0, the default, is
+of the next line; "k3c": the forward y pass on buddy-line CTA pairs); "t" marks the
+persistent form of the fused pass whose next tile's first-phase points are staged in
+tensor memory (one CTA per SM).  Variant 0, the default, is
 the fastest one measured on B200 at the sizes the table was tuned on; zm_plan_autotune
 re-measures them for a plan."""
 VARIANTS = {
@@ -21,7 +23,7 @@ VARIANTS = {
         (4, 4): [(1, 16, 256)], (4, 5): [(1, 8, 256)], (4, 6): [(1, 4, 256)], (2, 7): [(1, 8, 256), (1, 4, 128), (1, 16, 512)],
         (5, 6): [(1, 2, 256)], (5, 7): [(1, 1, 256), (2, 2, 256)], (4, 8): [(1, 1, 256), (2, 2, 256)],
         (5, 8): [(1, 1, 512), (2, 1, 256)], (6, 7): [(2, 1, 256), (1, 1, 512)],
-        (6, 8): [(2, 1, 512), (4, 1, 256), (4, 2, 512)],
+        (6, 8): [(2, 1, 512), (4, 1, 256), (4, 2, 512), (2, 1, 512, "t"), (4, 2, 512, "t")],
     },
 }
 # Out-of-place 2D forward configurations (used when the caller passes a workspace and the
@@ -32,7 +34,8 @@ VARIANTS = {
 # 1.81): 2.97 ms per forward transform against 4.61 for the in-place default.
 # complex128 (6, 8): the x pass on two-line tiles (clusters of four) writing the 2-row
 # interleave in whole 32-byte sectors (one-line tiles write each 16-byte element into a
-# sector of its own), the y pass on one-line tiles: 7.94 ms against 8.51.
+# sector of its own), the y pass on one-line tiles: 7.94 ms against 8.51.  (The
+# tensor-memory-staged forms are slower on the forward passes: y 3.29 -> 3.69 ms.)
 FWD_OOP = {
     "c64": {(6, 8): (7, 8, 3), (5, 8): (5, 5, 1), (6, 7): (2, 2, 1)},
     "c128": {(6, 8): (2, 0, 1)},
@@ -46,9 +49,12 @@ FWD_OOP = {
 # 128-byte line): 1.67 + 1.46 = 3.12 ms per inverse transform, against 3.24 for the
 # row-interleaved intermediate (8-element runs: 1.62 + 1.79; 16-byte runs: partial
 # sectors, 2.2 ms and up for the y pass).
+# complex128 (6, 8): both passes on the persistent tensor-memory-staged tiles (variant 3),
+# plain REPACK intermediate: 6.11 ms against 6.81 (the x pass, whose strided frequency-side
+# reads wait longest, 4.04 -> 3.39 ms; the y pass unchanged).
 INV_OOP = {
     "c64": {(6, 8): (7, 7, 2, "q")},
-    "c128": {},
+    "c128": {(6, 8): (3, 3, 0)},
 }
 T = {"c64": "float", "c128": "double"}
 for dt, table in VARIANTS.items():
@@ -66,6 +72,7 @@ for dt, table in VARIANTS.items():
             for vi, v in enumerate(vs):
                 cl, tl, nt = v[:3]
                 pers = "true" if len(v) > 3 and v[3] == "p" else "false"
+                tms = ", true" if len(v) > 3 and v[3] == "t" else ""
                 if len(v) > 3 and v[3] in ("k3", "k3p", "k3c"):
                     L.append(f"    case ({lv} << 16) | ({lm} << 8) | {vi}: "
                              f"return launch_k3<{lv}, {lm}, {'true' if inv else 'false'}, "
@@ -73,7 +80,7 @@ for dt, table in VARIANTS.items():
                              f"{'true' if v[3] == 'k3c' else 'false'}>(prm, st);")
                     continue
                 L.append(f"    case ({lv} << 16) | ({lm} << 8) | {vi}: "
-                         f"return launch_fused<{T[dt]}, {lv}, {lm}, {cl}, {tl}, {nt}, {'true' if inv else 'false'}, {pers}>(prm, st);")
+                         f"return launch_fused<{T[dt]}, {lv}, {lm}, {cl}, {tl}, {nt}, {'true' if inv else 'false'}, {pers}{tms}>(prm, st);")
         L += ["    default: break;", "    }", "    *handled = false;", "    return cudaSuccess;", "}", ""]
         if not inv:
             L += [f"int fused_variants_{dt}(int logvec, int logm) {{", "    switch ((logvec << 8) | logm) {"]

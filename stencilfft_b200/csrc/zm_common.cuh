@@ -89,6 +89,21 @@ template <> ZM_DEV cpx<float> ldg(const cpx<float> *p) {
     return {v.x, v.y};
 }
 
+// ------------------------------------------- per-thread asynchronous copies (cp.async)
+ZM_DEV void cp_async8(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                 "l"((unsigned long long)__cvta_generic_to_global(src))
+                 : "memory");
+}
+ZM_DEV void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                 "l"((unsigned long long)__cvta_generic_to_global(src))
+                 : "memory");
+}
+ZM_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+ZM_DEV void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+ZM_DEV void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }   // all but the newest group
+
 // ----------------------------------------------------- radix-R DFT codelets
 // Constant twiddles w_R^k = exp(DIR * 2 pi i k / R), DIR = -1 forward, +1 inverse.
 // cos(2 pi j / 32) for j = 0..8, the first octant of the 32-point circle.

@@ -91,6 +91,44 @@ ZM_DEV void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) 
                  : "memory");
 }
 constexpr unsigned long long kCopyWaitNs = 1000000000ull;   // 1 s
+// ------------------------------------------------ tensor memory (TMEM) staging
+// 128 lanes x 512 columns of 32 bits per SM.  With the 32x32b shape, warp w reaches the
+// 32 lanes 32 (w % 4) .. 32 (w % 4) + 31, lane i of the warp its own lane; an address is
+// (lane << 16) | column.  Every access is warp-wide (.sync.aligned).
+ZM_DEV void tmem_alloc(uint32_t *s_addr, unsigned ncols) {   // one warp
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(s_addr)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+ZM_DEV void tmem_dealloc(uint32_t taddr, unsigned ncols) {   // the allocating warp
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+ZM_DEV void tmem_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+ZM_DEV void tmem_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// 16 words of this thread to columns [c, c + 16) of its lane
+ZM_DEV void tmem_st16(uint32_t taddr, const uint32_t *w) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16};" ::"r"(taddr),
+        "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7]), "r"(w[8]), "r"(w[9]),
+        "r"(w[10]), "r"(w[11]), "r"(w[12]), "r"(w[13]), "r"(w[14]), "r"(w[15])
+        : "memory");
+}
+// waits for this thread's earlier TMEM stores, reads 16 words and waits for the read (in
+// one statement, so that no use of w can be scheduled before the data is there)
+ZM_DEV void tmem_ld16(uint32_t taddr, uint32_t *w) {
+    asm volatile(
+        "tcgen05.wait::st.sync.aligned;\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7]), "=r"(w[8]),
+          "=r"(w[9]), "=r"(w[10]), "=r"(w[11]), "=r"(w[12]), "=r"(w[13]), "=r"(w[14]), "=r"(w[15])
+        : "r"(taddr)
+        : "memory");
+}
+
 // hint: bring [src, src + bytes) into L2 (no completion to wait for); 16-byte aligned,
 // bytes a multiple of 16
 ZM_DEV void bulk_prefetch_l2(const void *src, unsigned bytes) {
@@ -195,7 +233,7 @@ constexpr int fused_min_blocks() {
     return by_smem < 1 ? 1 : (by_smem < by_threads ? by_smem : by_threads);
 }
 
-template <typename T, int LV, int LM, int CL, int TL, int NT, bool INV, bool PERS>
+template <typename T, int LV, int LM, int CL, int TL, int NT, bool INV, bool PERS, bool TMS = false>
 __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, INV, PERS>()))
     fused_pass_kernel(const LineParams prm) {
     using SG = SliceGeom<LV, LM, CL, TL, NT>;
@@ -218,17 +256,27 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
     Wt *sta = stm + M;                     // complex64: w_N^{a 2^TLO}, a < NTA
     Wt *stb = sta + SG::NTA;               // complex64: w_N^b, b < NTB
     __shared__ int64_t s_abase[TL], s_fbase[TL];
+    __shared__ int64_t s_abase_n[TL], s_fbase_n[TL];   // TMS: the CTA's next tile
+    __shared__ uint32_t s_tmem;                          // TMS: tensor-memory base address
     __shared__ uint64_t s_bar;
 
     int rank = 0;
     if constexpr (CL > 1) rank = (int)cooperative_groups::this_cluster().block_rank();
     const int n1_0 = rank * ML, k2_0 = rank * VL;   // first owned row / column
     const Geom &g = prm.g;
-    const int tid = threadIdx.x;
+    int tid = threadIdx.x;   // not const: the TMS tile loop re-derives it opaquely per tile
     const C *in = reinterpret_cast<const C *>(prm.in);
     C *out = reinterpret_cast<C *>(prm.out);
     // strides of the pass (the same for every line)
-    const LineAddr a0 = line_addr(g, prm.kind, 0, prm.lg_inter);
+    // (TMS: the pass's address form lives in shared memory, read where used, so that the
+    // persistent tile loop does not hold it in registers)
+    __shared__ LineAddr s_a0;
+    const LineAddr a0r = line_addr(g, prm.kind, 0, prm.lg_inter);
+    if constexpr (TMS) {
+        if (tid == 0) s_a0 = a0r;
+        __syncthreads();
+    }
+    const LineAddr &a0 = TMS ? s_a0 : a0r;
     {
         const Wt *tv = reinterpret_cast<const Wt *>(prm.twv);
         const Wt *tm = reinterpret_cast<const Wt *>(prm.twm);
@@ -247,6 +295,13 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
             s_fbase[tid] = a.f_base;
         }
     };
+    auto set_next = [&](int64_t l0) {   // TMS
+        if (tid < TL) {
+            const LineAddr a = line_addr(g, prm.kind, l0 + tid, prm.lg_inter);
+            s_abase_n[tid] = a.a_base;
+            s_fbase_n[tid] = a.f_base;
+        }
+    };
     const int logL = g.logL, logVP = g.logVP;
     const int64_t L = g.L, VP = g.vp;
     const bool scl = prm.apply_scale != 0;
@@ -256,15 +311,16 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
     static_assert(VPT * VE * NT == E, "vector copy");
 
     // frequency side: pointer to (t, k2 global, k1 = k1_0) and the step between k1 and k1 + kstep
-    const int flg = a0.f_lg;
-    auto fptr = [&](auto *base, int t, int k2, int k1_0) {
+    auto fptr_b = [&](auto *base, const int64_t *fb, int t, int k2, int k1_0) {
         const int64_t c = k2 >> logVP, f = k2 & (VP - 1);
         const int64_t pos = (int64_t)k1_0 * VP + f;
-        return base + s_fbase[t] + c * a0.f_chunk + (pos >> flg) * a0.f_hi + (pos & ((1 << flg) - 1));
+        return base + fb[t] + c * a0.f_chunk + (pos >> a0.f_lg) * a0.f_hi + (pos & ((1 << a0.f_lg) - 1));
     };
+    auto fptr = [&](auto *base, int t, int k2, int k1_0) { return fptr_b(base, s_fbase, t, k2, k1_0); };
     // (VP is a multiple of the interleave 2^flg whenever flg > 0)
-    const int64_t fstep1 = (((int64_t)RC2 * VP) >> flg) * a0.f_hi;   // k1 += RC2 (column stage 1)
-    const int64_t fstep2 = (((int64_t)RC1 * VP) >> flg) * a0.f_hi;   // k1 += RC1 (column stage 2)
+    // k1 += RC2 (column stage 1) / RC1 (column stage 2), recomputed where used
+    auto fstep1 = [&]() -> int64_t { return (((int64_t)RC2 * VP) >> a0.f_lg) * a0.f_hi; };
+    auto fstep2 = [&]() -> int64_t { return (((int64_t)RC1 * VP) >> a0.f_lg) * a0.f_hi; };
     // vector-side element e of this CTA's rows (row-major over [t][n1l][p]) -> global
     // (16-byte vector copies; used only where the vector side is contiguous, a_pos = 1)
     auto aaddr = [&](int e) {
@@ -275,10 +331,11 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
     // vector side: global offset of the first element of local row n1l of line t;
     // consecutive positions of a row are a_pos apart
     const int64_t apos = a0.a_pos;
-    auto arow = [&](int t, int n1l) {
+    auto arow_b = [&](const int64_t *ab, int t, int n1l) {
         const int r = (n1_0 + n1l) * VEC;
-        return s_abase[t] + (int64_t)(r >> logL) * a0.a_chunk + (int64_t)(r & (L - 1)) * apos;
+        return ab[t] + (int64_t)(r >> logL) * a0.a_chunk + (int64_t)(r & (L - 1)) * apos;
     };
+    auto arow = [&](int t, int n1l) { return arow_b(s_abase, t, n1l); };
     // Lane orders.  Rows: (j, n1, t) -- or t first when the vector side interleaves
     // lines (apos > 1) so that the lines' elements pair up in memory.  Columns:
     // (k2, j, t) -- or (low interleave bits of k2, t, rest of k2, j) when the frequency
@@ -300,6 +357,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
     };
     auto colunit = [&](int u, int nj, int &t, int &k2l, int &j) {
         if (tfirst_cols) {
+            const int flg = a0.f_lg;
             const int gm = (1 << flg) - 1;
             const int lo = u & gm;
             const int rr = u >> flg;
@@ -402,7 +460,8 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
     };
 
     // ---- forward: w_N^{n1 k2}, M-point column transforms over n1, frequency-side store
-    auto fwd_columns = [&]() {
+    // hook(2) runs between the two column stages (TMS prefetch; a no-op otherwise)
+    auto fwd_columns = [&](auto &&hook) {
       if constexpr (SG::template colq<T>()) {
         // complex64, one CTA per tile, RC2 = 16: the first stage runs with lanes along
         // j = n1 mod RC2 (k2 = zk with CL = 1); unit (t, k2, j) transforms n1 = j + RC2 r,
@@ -435,6 +494,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
 #pragma unroll
             for (int r = 0; r < RC1; r++) S[SG::Y(zt[i], zk[i], r * RC2 + zj[i])] = z[i][r];
         __syncthreads();
+        hook(2);
         constexpr int NU2 = EPT / RC2;
 #pragma unroll
         for (int i = 0; i < NU2; i++) {
@@ -449,7 +509,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
             dft<RC2, DIR, T>(y);
             C *op = fptr(out, t, k2l, j2);
 #pragma unroll
-            for (int r = 0; r < RC2; r++) op[fstep2 * r] = scale_c(y[r]);
+            for (int r = 0; r < RC2; r++) op[fstep2() * r] = scale_c(y[r]);
         }
       } else {
         constexpr int NU = EPT / RC1;
@@ -478,7 +538,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
             for (int i = 0; i < NU; i++) {
                 C *op = fptr(out, zt[i], k2_0 + zk[i], 0);
 #pragma unroll
-                for (int r = 0; r < RC1; r++) op[fstep1 * r] = scale_c(z[i][r]);
+                for (int r = 0; r < RC1; r++) op[fstep1() * r] = scale_c(z[i][r]);
             }
         } else {
             __syncthreads();
@@ -487,6 +547,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
 #pragma unroll
                 for (int r = 0; r < RC1; r++) S[SG::Y(zt[i], zk[i], zj[i] * RC1 + r)] = z[i][r];
             __syncthreads();
+            hook(2);
             constexpr int NU2 = EPT / RC2;
 #pragma unroll
             for (int i = 0; i < NU2; i++) {
@@ -501,7 +562,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
                 dft<RC2, DIR, T>(y);
                 C *op = fptr(out, t, k2_0 + k2l, j2);
 #pragma unroll
-                for (int r = 0; r < RC2; r++) op[fstep2 * r] = scale_c(y[r]);
+                for (int r = 0; r < RC2; r++) op[fstep2() * r] = scale_c(y[r]);
             }
         }
       }
@@ -580,10 +641,10 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
             if (!copies_lost && tile + ncl < ntiles) issue(tile + ncl);
             fwd_row_stage2_scatter();
             tile_sync<CL>();
-            fwd_columns();
+            fwd_columns([](int) {});
         }
         return;
-    } else {
+    } else if constexpr (!TMS) {
         set_tile((int64_t)(blockIdx.x / CL) * TL);
         // forward: L2 prefetch of the vector side of the tile one wave of clusters ahead,
         // so its HBM reads overlap this tile's work (for an interleaved intermediate the
@@ -608,19 +669,127 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
         __syncthreads();
     }
 
+    // ---- TMS (tensor-memory staging): the grid is persistent and each CTA walks tiles
+    //      c, c + clusters, ...  The EPT points a thread loads from global memory first in a
+    //      tile (vector-side rows forward, frequency-side columns inverse) are, for its NEXT
+    //      tile, fetched during the current one in NCH chunks of 16 words: asynchronous
+    //      copies (cp.async, no registers held) into a two-slot shared-memory ring behind
+    //      the slice, chunks 0 and 1 at phase boundary 0 of the tile and chunk k >= 2 at
+    //      boundary k - 1; a chunk is moved on into this thread's columns of tensor memory
+    //      one boundary after its copy was issued (k + 1), freeing its slot; the last one
+    //      is read from its slot when the next tile starts, the others from tensor memory.
+    //      So the tile's HBM reads overlap the previous tile's work.  One CTA per SM (the
+    //      slice fills shared memory), so the NCOLS columns are free at once.
+    constexpr int WPP = (int)sizeof(C) / 4;                // 32-bit words per point
+    constexpr int PC = 16 / WPP;                           // points per chunk
+    constexpr int NCH = EPT / PC;                          // chunks per thread
+    constexpr int NCOLS = EPT * WPP * (NT / 128);          // columns of the CTA
+    if constexpr (TMS) {
+        static_assert(!PERS && (INV || RA2 > 1) && RC2 > 1 && (!INV || RA2 > 1), "TMS tile shape");
+        static_assert(NCH >= 2 && NCH <= 4, "TMS chunk schedule: at most one move per phase boundary");
+        static_assert(NT % 128 == 0 && NCOLS >= 32 && NCOLS <= 512 && (NCOLS & (NCOLS - 1)) == 0, "TMEM columns");
+        static_assert(2 * (fused_smem_bytes<T, LV, LM, CL, TL, NT, INV, PERS>() + 1024) > 228 * 1024,
+                      "TMS needs one CTA per SM");
+    }
+    const int warp = tid >> 5;
+    // ring slot s, point q of this thread (thread-fastest: conflict-free 8 / 16-byte accesses)
+    C *ring = reinterpret_cast<C *>(smem_raw + fused_smem_bytes<T, LV, LM, CL, TL, NT, INV, PERS>());
+    auto ring_at = [&](int slot, int q) { return ring + ((size_t)slot * PC + q) * NT + tid; };
+    bool has_next = false;                                 // block-uniform
+    auto chunk_src = [&](int c, int q) -> const C * {      // point q of chunk c, next tile
+        const int f = c * PC + q;
+        if constexpr (!INV) {
+            int t, n1l, j;
+            rowunit(tid + (f / RA1) * NT, RA2, t, n1l, j);
+            return in + arow_b(s_abase_n, t, n1l) + j * apos + RA2 * (f % RA1) * apos;
+        } else {
+            int t, k2l, j;
+            colunit(tid + (f / RC1) * NT, RC2, t, k2l, j);
+            return fptr_b(in, s_fbase_n, t, k2_0 + k2l, j) + fstep1() * (f % RC1);
+        }
+    };
+    auto tm_addr = [&](int c) -> uint32_t {
+        return s_tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * EPT * WPP + c * 16);
+    };
+    auto issue_chunk = [&](int c) {                        // copies into slot c & 1, one group
+#pragma unroll
+        for (int q = 0; q < PC; q++) {
+            if constexpr (sizeof(C) == 16) cp_async16(ring_at(c & 1, q), chunk_src(c, q));
+            else cp_async8(ring_at(c & 1, q), chunk_src(c, q));
+        }
+        cp_async_commit();
+    };
+    auto move_chunk = [&](int c) {                         // slot c & 1 -> tensor memory
+        cp_async_wait_one();                               // all groups but the newest landed
+        uint32_t w[16];
+#pragma unroll
+        for (int q = 0; q < PC; q++) memcpy(w + q * WPP, ring_at(c & 1, q), sizeof(C));
+        tmem_st16(tm_addr(c), w);
+    };
+    auto hook = [&](int k) {
+        if constexpr (TMS) {
+            if (!has_next) return;
+            if (k == 0) {
+                issue_chunk(0);
+                issue_chunk(1);
+            } else if (k - 1 <= NCH - 2) {
+                move_chunk(k - 1);
+                if (k + 1 < NCH) issue_chunk(k + 1);
+            }
+        }
+    };
+    auto tms_read = [&](C *dst) {   // this tile's EPT first-phase points, flat order
+#pragma unroll
+        for (int c = 0; c < NCH - 1; c++) {
+            uint32_t w[16];
+            tmem_ld16(tm_addr(c), w);
+            memcpy(dst + c * PC, w, 64);
+        }
+        cp_async_wait_all();
+#pragma unroll
+        for (int q = 0; q < PC; q++) dst[(NCH - 1) * PC + q] = *ring_at((NCH - 1) & 1, q);
+    };
+    if constexpr (TMS) {
+        if (warp == 0) tmem_alloc(&s_tmem, NCOLS);
+        tmem_fence_before();
+        __syncthreads();
+        tmem_fence_after();
+    }
+    const int64_t tms_ntiles = prm.nlines / TL, tms_ncl = gridDim.x / CL;
+    int64_t tms_tile = blockIdx.x / CL;
+    bool tms_first = true;
+    for (;;) {
+    if constexpr (TMS) {
+        if (tms_tile >= tms_ntiles) break;
+        // an opaque copy of tid: the per-thread index and address arithmetic of the tile is
+        // then recomputed in every tile instead of being hoisted out of the loop and held
+        // in registers across it (which spilled 380-460 bytes at 128 registers)
+        asm volatile("mov.u32 %0, %0;" : "+r"(tid));
+        __syncthreads();   // the previous tile is done with S and the bases
+        set_tile(tms_tile * TL);
+        has_next = tms_tile + tms_ncl < tms_ntiles;
+        if (has_next) set_next((tms_tile + tms_ncl) * TL);
+        __syncthreads();
+    }
     if constexpr (!INV && RA2 > 1) {
         // ================= forward, two row stages, one tile per cluster: the first row
-        // stage reads the vector side straight from global memory
+        // stage reads the vector side straight from global memory (TMS: from tensor
+        // memory after the CTA's first tile)
         {
             constexpr int NU = EPT / RA1;
             C v[NU][RA1];
             int ut[NU], un1[NU], uj[NU];
 #pragma unroll
-            for (int i = 0; i < NU; i++) {
-                rowunit(tid + i * NT, RA2, ut[i], un1[i], uj[i]);
-                const C *row = in + arow(ut[i], un1[i]) + uj[i] * apos;
+            for (int i = 0; i < NU; i++) rowunit(tid + i * NT, RA2, ut[i], un1[i], uj[i]);
+            if (TMS && !tms_first) {
+                tms_read(&v[0][0]);
+            } else {
 #pragma unroll
-                for (int r = 0; r < RA1; r++) v[i][r] = ldg(row + RA2 * r * apos);
+                for (int i = 0; i < NU; i++) {
+                    const C *row = in + arow(ut[i], un1[i]) + uj[i] * apos;
+#pragma unroll
+                    for (int r = 0; r < RA1; r++) v[i][r] = ldg(row + RA2 * r * apos);
+                }
             }
 #pragma unroll
             for (int i = 0; i < NU; i++) {
@@ -630,9 +799,12 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
             }
         }
         __syncthreads();
+        hook(0);
         fwd_row_stage2_scatter();
         tile_sync<CL>();
-        fwd_columns();
+        hook(1);
+        fwd_columns(hook);
+        hook(3);
     } else if constexpr (!INV) {
         // ================= forward, one row stage (RA2 == 1): one tile per cluster
         // ---- 1. vector side -> local rows X (16-byte vectors, all loads before stores)
@@ -677,7 +849,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
         }
         tile_sync<CL>();
         // ---- 3. columns
-        fwd_columns();
+        fwd_columns([](int) {});
     } else {
         // ================= inverse: one tile per cluster
         // ---- 1. frequency side -> M-point inverse column transforms over k1 (local columns)
@@ -686,12 +858,16 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
             C z[NU][RC1];
             int zt[NU], zk[NU], zj[NU];
 #pragma unroll
-            for (int i = 0; i < NU; i++) {
-                const int u = tid + i * NT;
-                colunit(u, RC2, zt[i], zk[i], zj[i]);
-                const C *ip = fptr(in, zt[i], k2_0 + zk[i], zj[i]);
+            for (int i = 0; i < NU; i++) colunit(tid + i * NT, RC2, zt[i], zk[i], zj[i]);
+            if (TMS && !tms_first) {
+                tms_read(&z[0][0]);
+            } else {
 #pragma unroll
-                for (int r = 0; r < RC1; r++) z[i][r] = ldg(ip + fstep1 * r);
+                for (int i = 0; i < NU; i++) {
+                    const C *ip = fptr(in, zt[i], k2_0 + zk[i], zj[i]);
+#pragma unroll
+                    for (int r = 0; r < RC1; r++) z[i][r] = ldg(ip + fstep1() * r);
+                }
             }
 #pragma unroll
             for (int i = 0; i < NU; i++) dft<RC1, DIR, T>(z[i]);
@@ -712,6 +888,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
 #pragma unroll
                     for (int r = 0; r < RC1; r++) S[SG::Y(zt[i], zk[i], zj[i] * RC1 + r)] = z[i][r];
                 __syncthreads();
+                hook(0);
                 constexpr int NU2 = EPT / RC2;
                 C y[NU2][RC2];
                 int yt[NU2], yk[NU2], yj[NU2];
@@ -745,6 +922,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
             }
         }
         tile_sync<CL>();
+        hook(1);
         // ---- 2. VEC-point inverse row transforms over k2 -> local rows X[t][n1l][n2]
         {
             constexpr int NU = EPT / RA1;
@@ -769,6 +947,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
                 for (int r = 0; r < RA1; r++) S[SG::X(ut[i], un1[i], uj[i] * RA1 + r)] = v[i][r];
             if constexpr (RA2 > 1) {
                 __syncthreads();
+                hook(2);
                 constexpr int NU2 = EPT / RA2;
                 C w[NU2][RA2];
                 int wt[NU2], wn1[NU2], wj[NU2];
@@ -809,6 +988,20 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
                 *reinterpret_cast<uint4 *>(out + aaddr(e)) = v;
             }
         }
+        hook(3);
+    }
+    if constexpr (!TMS) break;
+    tms_first = false;
+    tms_tile += tms_ncl;
+    }   // tile loop (one pass unless TMS)
+    if constexpr (TMS) {
+        cp_async_wait_all();   // nothing in flight when the CTA exits
+        tmem_fence_before();
+        __syncthreads();   // every tensor-memory access of the CTA is complete
+        if (warp == 0) {
+            tmem_fence_after();
+            tmem_dealloc(s_tmem, NCOLS);
+        }
     }
 }
 
@@ -838,18 +1031,20 @@ static int resident_clusters(K kern, size_t smem, int dev) {
     return n;
 }
 
-template <typename T, int LV, int LM, int CL, int TL, int NT, bool INV, bool PERS = false>
+template <typename T, int LV, int LM, int CL, int TL, int NT, bool INV, bool PERS = false, bool TMS = false>
 cudaError_t launch_fused(const LineParams &prm, cudaStream_t st) {
-    constexpr size_t smem = fused_smem_bytes<T, LV, LM, CL, TL, NT, INV, PERS>();
+    // TMS: the two-slot ring of 16-word chunks behind the slice
+    constexpr size_t smem = fused_smem_bytes<T, LV, LM, CL, TL, NT, INV, PERS>() + (TMS ? (size_t)2 * 64 * NT : 0);
     static_assert(smem <= 227 * 1024, "shared memory of one CTA");
-    constexpr bool persistent = fused_persistent<T, LV, LM, CL, TL, NT, INV, PERS>();
+    constexpr bool bulk_persistent = fused_persistent<T, LV, LM, CL, TL, NT, INV, PERS>();
+    constexpr bool persistent = TMS || bulk_persistent;
     if (prm.inter_q) return cudaErrorInvalidValue;   // row-interleaved intermediates only
     // the staging rows of a persistent pass hold sg = 1, 2 or 4 interleaved lines and
     // are sized for sg <= TL: a wider interleave of the y pass's vector side is refused
-    if (persistent && prm.kind == PASS_Y2 && prm.lg_inter > 0 &&
+    if (bulk_persistent && prm.kind == PASS_Y2 && prm.lg_inter > 0 &&
         ((1 << prm.lg_inter) > TL || prm.lg_inter > 2))
         return cudaErrorInvalidValue;
-    auto kern = fused_pass_kernel<T, LV, LM, CL, TL, NT, INV, PERS>;
+    auto kern = fused_pass_kernel<T, LV, LM, CL, TL, NT, INV, PERS, TMS>;
     static int attr_done[64], clusters[64];
     int dev = 0;
     cudaGetDevice(&dev);

@@ -28,6 +28,8 @@ cudaError_t launch_fused_c128_fwd(const LineParams &prm, cudaStream_t st, bool *
     case (6 << 16) | (8 << 8) | 0: return launch_fused<double, 6, 8, 2, 1, 512, false, false>(prm, st);
     case (6 << 16) | (8 << 8) | 1: return launch_fused<double, 6, 8, 4, 1, 256, false, false>(prm, st);
     case (6 << 16) | (8 << 8) | 2: return launch_fused<double, 6, 8, 4, 2, 512, false, false>(prm, st);
+    case (6 << 16) | (8 << 8) | 3: return launch_fused<double, 6, 8, 2, 1, 512, false, false, true>(prm, st);
+    case (6 << 16) | (8 << 8) | 4: return launch_fused<double, 6, 8, 4, 2, 512, false, false, true>(prm, st);
     default: break;
     }
     *handled = false;
@@ -45,7 +47,7 @@ int fused_variants_c128(int logvec, int logm) {
     case (4 << 8) | 8: return 2;
     case (5 << 8) | 8: return 2;
     case (6 << 8) | 7: return 2;
-    case (6 << 8) | 8: return 3;
+    case (6 << 8) | 8: return 5;
     default: return 0;
     }
 }
@@ -55,6 +57,7 @@ int fused_interleave_lg_c128(int logvec, int logm, int variant) {
     case (5 << 16) | (6 << 8) | 0: return 1;
     case (5 << 16) | (7 << 8) | 1: return 1;
     case (6 << 16) | (8 << 8) | 2: return 1;
+    case (6 << 16) | (8 << 8) | 4: return 1;
     default: return 0;
     }
 }
@@ -68,6 +71,7 @@ int fused_fwd_oop_c128(int logvec, int logm, int *vx, int *vy, int *lg, int *qin
 
 int fused_inv_oop_c128(int logvec, int logm, int *vx, int *vy, int *lg, int *qint) {
     switch ((logvec << 8) | logm) {
+    case (6 << 8) | 8: *vx = 3; *vy = 3; *lg = 0; *qint = 0; return 1;
     default: return 0;
     }
 }

@@ -28,6 +28,8 @@ cudaError_t launch_fused_c128_inv(const LineParams &prm, cudaStream_t st, bool *
     case (6 << 16) | (8 << 8) | 0: return launch_fused<double, 6, 8, 2, 1, 512, true, false>(prm, st);
     case (6 << 16) | (8 << 8) | 1: return launch_fused<double, 6, 8, 4, 1, 256, true, false>(prm, st);
     case (6 << 16) | (8 << 8) | 2: return launch_fused<double, 6, 8, 4, 2, 512, true, false>(prm, st);
+    case (6 << 16) | (8 << 8) | 3: return launch_fused<double, 6, 8, 2, 1, 512, true, false, true>(prm, st);
+    case (6 << 16) | (8 << 8) | 4: return launch_fused<double, 6, 8, 4, 2, 512, true, false, true>(prm, st);
     default: break;
     }
     *handled = false;

@@ -47,18 +47,6 @@ struct K3Geom {
     static ZM_DEV int s2(int kb, int d0, int ka) { return kb * R2 + d0 * 17 + ka; }
 };
 
-ZM_DEV void cp_async8(void *dst, const void *src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
-                 "l"((unsigned long long)__cvta_generic_to_global(src))
-                 : "memory");
-}
-ZM_DEV void cp_async16(void *dst, const void *src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
-                 "l"((unsigned long long)__cvta_generic_to_global(src))
-                 : "memory");
-}
-ZM_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-ZM_DEV void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 ZM_DEV void prefetch_l2_bytes(const void *p, int64_t bytes) {
     const unsigned char *src = reinterpret_cast<const unsigned char *>(p);
     if (((uintptr_t)src & 15) != 0 || (bytes & 15) != 0) return;

@@ -151,3 +151,27 @@ def test_headline_stencils_against_roll(dt):
     for o, w in ((lap, want[0]), (gx, want[1]), (gy, want[2])):
         pl.real_to_natural(o, natout)
         assert _norm(natout.view(N, N) - w) / _norm(w) < tol
+
+
+def test_headline_c128_every_tile_variant():
+    """Every complex128 tile shape of the 2^14-point lines (clusters of two / four, one or
+    two lines per tile, and their persistent forms staging the next tile in tensor memory)
+    gives the default configuration's spectrum, in place (no workspace), and returns the
+    field."""
+    import torch
+    from stencilfft_b200 import Plan
+    pl = Plan(2, N, B, P, dtype="c128")
+    u = _field(pl, "gauss")
+    a, want, got = pl.empty(), pl.empty(), pl.empty()
+    work = pl.empty()
+    pl.forward_fft(u, want, work=work)            # default: out of place
+    del work
+    for v in range(pl.kernel_variants):
+        pl.set_kernel_variant(v)
+        a.copy_(u)
+        pl.forward_fft(a, got)                    # in place on the variant's tiles
+        assert _norm(got - want) / _norm(want) < 1e-14, v
+        a.copy_(got)
+        pl.inverse_fft(a, got, scale=1.0 / (N * N))
+        assert _norm(got - u) / _norm(u) < 1e-12, v
+        assert pl.device_status() == 0
