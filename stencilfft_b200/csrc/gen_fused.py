@@ -32,13 +32,15 @@ VARIANTS = {
 # x pass on the persistent three-stage kernel (1.21 ms), y pass on buddy-line CTA pairs
 # of the three-stage kernel reading the 8-row interleave (1.77 ms; one line per CTA
 # 1.81): 2.97 ms per forward transform against 4.61 for the in-place default.
-# complex128 (6, 8): the x pass on two-line tiles (clusters of four) writing the 2-row
-# interleave in whole 32-byte sectors (one-line tiles write each 16-byte element into a
-# sector of its own), the y pass on one-line tiles: 7.94 ms against 8.51.  (The
-# tensor-memory-staged forms are slower on the forward passes: y 3.29 -> 3.69 ms.)
+# complex128 (6, 8): a 16-row interleave (G = VP), so that the x pass on one-line tiles
+# writes runs of 16 elements (256 bytes) -- with the plain layout it wrote each 16-byte
+# element into a 32-byte sector of its own (5.16 ms) -- and the y pass reads its line 16
+# elements apart on the persistent tensor-memory-staged tiles (variant 3), which hide the
+# wait for those scattered reads: x 3.30 + y 3.70 = 6.97 ms per forward transform, against
+# 7.86 (two-line x tiles on clusters of four writing the 2-row interleave) and 8.51.
 FWD_OOP = {
     "c64": {(6, 8): (7, 8, 3), (5, 8): (5, 5, 1), (6, 7): (2, 2, 1)},
-    "c128": {(6, 8): (2, 0, 1)},
+    "c128": {(6, 8): (0, 3, 4)},
 }
 # Out-of-place 2D inverse configurations (caller workspace, default variant): y pass
 # variant (frequency side -> work), x pass variant (work -> vector side), log2 of the

@@ -924,6 +924,13 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
         tile_sync<CL>();
         hook(1);
         // ---- 2. VEC-point inverse row transforms over k2 -> local rows X[t][n1l][n2]
+        //      (one row stage, RA2 == 1: each row is one thread's alone, read as 16-byte
+        //      vectors where the row stride allows, and with a contiguous vector side stored
+        //      straight from registers -- no barrier, no shared-memory write-back)
+        constexpr bool ROWVEC = RA2 == 1 && (RA1 * sizeof(C)) % 16 == 0 && (SG::XR * sizeof(C)) % 16 == 0;
+        // (complex64 only: complex128 rows of 64 bytes stored by one lane each were slower
+        // than the coalesced 16-byte sweep of section 3, 3D N = 512 inverse 4.09 -> 4.17 ms)
+        const bool rows_direct = RA2 == 1 && sizeof(C) == 8 && (RA1 * sizeof(C)) % 16 == 0 && apos == 1;
         {
             constexpr int NU = EPT / RA1;
             C v[NU][RA1];
@@ -935,16 +942,39 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
                 const int rr = u / RA2;
                 un1[i] = rr % ML;
                 ut[i] = rr / ML;
+                if constexpr (ROWVEC) {
+                    const uint4 *rp = reinterpret_cast<const uint4 *>(&S[SG::X(ut[i], un1[i], 0)]);
 #pragma unroll
-                for (int r = 0; r < RA1; r++) v[i][r] = S[SG::X(ut[i], un1[i], uj[i] + RA2 * r)];
+                    for (int q = 0; q < RA1 * (int)sizeof(C) / 16; q++)
+                        *reinterpret_cast<uint4 *>(&v[i][q * 16 / (int)sizeof(C)]) = rp[q];
+                } else {
+#pragma unroll
+                    for (int r = 0; r < RA1; r++) v[i][r] = S[SG::X(ut[i], un1[i], uj[i] + RA2 * r)];
+                }
             }
-            __syncthreads();
+            if constexpr (RA2 > 1) __syncthreads();
 #pragma unroll
             for (int i = 0; i < NU; i++) dft<RA1, DIR, T>(v[i]);
+            if (rows_direct) {
+                // row (t, n1) of the vector side: VEC consecutive positions, 16-byte aligned
 #pragma unroll
-            for (int i = 0; i < NU; i++)
+                for (int i = 0; i < NU; i++) {
+                    C *row = out + arow(ut[i], un1[i]);
 #pragma unroll
-                for (int r = 0; r < RA1; r++) S[SG::X(ut[i], un1[i], uj[i] * RA1 + r)] = v[i][r];
+                    for (int r = 0; r < RA1; r++) {
+                        const C o = v[i][r];
+                        v[i][r] = scl ? C{sre * o.x - sim * o.y, sre * o.y + sim * o.x} : o;
+                    }
+#pragma unroll
+                    for (int q = 0; q < RA1 * (int)sizeof(C) / 16; q++)
+                        reinterpret_cast<uint4 *>(row)[q] = *reinterpret_cast<const uint4 *>(&v[i][q * 16 / (int)sizeof(C)]);
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < NU; i++)
+#pragma unroll
+                    for (int r = 0; r < RA1; r++) S[SG::X(ut[i], un1[i], uj[i] * RA1 + r)] = v[i][r];
+            }
             if constexpr (RA2 > 1) {
                 __syncthreads();
                 hook(2);
@@ -970,8 +1000,10 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
                 }
             }
         }
-        // ---- 3. single row stage: local rows -> vector side (16-byte vectors), scale applied here
+        // ---- 3. single row stage, strided vector side: local rows -> vector side (16-byte
+        //      vectors), scale applied here
         if constexpr (RA2 == 1) {
+          if (!rows_direct) {
             __syncthreads();
 #pragma unroll
             for (int i = 0; i < VPT; i++) {
@@ -987,6 +1019,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
                 }
                 *reinterpret_cast<uint4 *>(out + aaddr(e)) = v;
             }
+          }
         }
         hook(3);
     }

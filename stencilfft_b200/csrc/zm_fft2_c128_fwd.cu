@@ -64,7 +64,7 @@ int fused_interleave_lg_c128(int logvec, int logm, int variant) {
 
 int fused_fwd_oop_c128(int logvec, int logm, int *vx, int *vy, int *lg, int *qint) {
     switch ((logvec << 8) | logm) {
-    case (6 << 8) | 8: *vx = 2; *vy = 0; *lg = 1; *qint = 0; return 1;
+    case (6 << 8) | 8: *vx = 0; *vy = 3; *lg = 4; *qint = 0; return 1;
     default: return 0;
     }
 }
