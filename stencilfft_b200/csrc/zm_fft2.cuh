@@ -159,6 +159,13 @@ template <int LV, int LM, int CL, int TL, int NT> struct SliceGeom {
     static constexpr int XE = TL * ML * XR, YE = TL * VL * YR;
     static constexpr int ELEMS = XE > YE ? XE : YE;
     static ZM_DEV int X(int t, int n1l, int p) { return (t * ML + n1l) * XR + p + (PADX ? p / RA1 : 0); }
+    // rows of the inverse with one row stage (RA2 == 1) where every access is per element
+    // or the element is 16 bytes: an odd stride VEC + 1, so that the column stage's
+    // scatter, with lanes along 16 consecutive rows of one column, hits 16 distinct bank
+    // pairs (the stride VEC + 2 of the 16-byte row reads repeats every 8 rows)
+    static constexpr int XRI = VEC + 1;
+    static_assert(PADX || XRI <= XR, "the odd-stride rows fit the slice");
+    static ZM_DEV int XI(int t, int n1l, int p) { return (t * ML + n1l) * XRI + p; }
     // Column position swizzle for VEC <= 4 tiles of several lines: where lanes run over the
     // lines t first (a strided frequency side), lines t and t + 4 would sit on the same bank
     // pairs (their rows are 4 YR = 0 mod 16 words apart); q ^ ysw(t) spreads the eight
@@ -852,6 +859,11 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
         fwd_columns([](int) {});
     } else {
         // ================= inverse: one tile per cluster
+        // rows X in the odd-stride form (SliceGeom::XI) where nothing reads them as 16-byte
+        // vectors of several elements: complex128, or complex64 rows stored straight to a
+        // contiguous vector side (block-uniform)
+        const bool xri = RA2 == 1 && (sizeof(C) == 16 || ((RA1 * sizeof(C)) % 16 == 0 && apos == 1));
+        auto Xs = [&](int t, int n1l, int p) { return xri ? SG::XI(t, n1l, p) : SG::X(t, n1l, p); };
         // ---- 1. frequency side -> M-point inverse column transforms over k1 (local columns)
         {
             constexpr int NU = EPT / RC1;
@@ -880,7 +892,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
                     Walk wk = walk(0, 1, k2);                            // n1 = r
 #pragma unroll
                     for (int r = 0; r < RC1; r++)
-                        xowner(r)[SG::X(zt[i], r % ML, k2)] = wk.apply(z[i][r], true);
+                        xowner(r)[Xs(zt[i], r % ML, k2)] = wk.apply(z[i][r], true);
                 }
             } else {
 #pragma unroll
@@ -895,10 +907,17 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
 #pragma unroll
                 for (int i = 0; i < NU2; i++) {
                     const int u = tid + i * NT;
-                    yk[i] = u % VL;
-                    const int rr = u / VL;
-                    yj[i] = rr % RC1;
-                    yt[i] = rr / RC1;
+                    if (xri) {   // lanes along the rows yj of one column (the scatter below)
+                        yj[i] = u % RC1;
+                        const int rr = u / RC1;
+                        yk[i] = rr % VL;
+                        yt[i] = rr / VL;
+                    } else {
+                        yk[i] = u % VL;
+                        const int rr = u / VL;
+                        yj[i] = rr % RC1;
+                        yt[i] = rr / RC1;
+                    }
 #pragma unroll
                     for (int r = 0; r < RC2; r++) y[i][r] = S[SG::Y(yt[i], yk[i], yj[i] + RC1 * r)];
                 }
@@ -916,7 +935,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
 #pragma unroll
                     for (int r = 0; r < RC2; r++) {
                         const int n1 = yj[i] + RC1 * r;
-                        xowner(n1)[SG::X(yt[i], n1 % ML, k2)] = wk.apply(y[i][r], true);
+                        xowner(n1)[Xs(yt[i], n1 % ML, k2)] = wk.apply(y[i][r], true);
                     }
                 }
             }
@@ -942,14 +961,14 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
                 const int rr = u / RA2;
                 un1[i] = rr % ML;
                 ut[i] = rr / ML;
-                if constexpr (ROWVEC) {
-                    const uint4 *rp = reinterpret_cast<const uint4 *>(&S[SG::X(ut[i], un1[i], 0)]);
+                if (ROWVEC && !(xri && sizeof(C) < 16)) {
+                    const uint4 *rp = reinterpret_cast<const uint4 *>(&S[Xs(ut[i], un1[i], 0)]);
 #pragma unroll
                     for (int q = 0; q < RA1 * (int)sizeof(C) / 16; q++)
                         *reinterpret_cast<uint4 *>(&v[i][q * 16 / (int)sizeof(C)]) = rp[q];
                 } else {
 #pragma unroll
-                    for (int r = 0; r < RA1; r++) v[i][r] = S[SG::X(ut[i], un1[i], uj[i] + RA2 * r)];
+                    for (int r = 0; r < RA1; r++) v[i][r] = S[Xs(ut[i], un1[i], uj[i] + RA2 * r)];
                 }
             }
             if constexpr (RA2 > 1) __syncthreads();
@@ -973,7 +992,7 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
 #pragma unroll
                 for (int i = 0; i < NU; i++)
 #pragma unroll
-                    for (int r = 0; r < RA1; r++) S[SG::X(ut[i], un1[i], uj[i] * RA1 + r)] = v[i][r];
+                    for (int r = 0; r < RA1; r++) S[Xs(ut[i], un1[i], uj[i] * RA1 + r)] = v[i][r];
             }
             if constexpr (RA2 > 1) {
                 __syncthreads();
@@ -1008,7 +1027,8 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
 #pragma unroll
             for (int i = 0; i < VPT; i++) {
                 const int e = (tid + i * NT) * VE;
-                uint4 v = *reinterpret_cast<const uint4 *>(&S[xidx_of_e(e)]);
+                const int et = e / (ML * VEC), er = e % (ML * VEC);
+                uint4 v = *reinterpret_cast<const uint4 *>(&S[Xs(et, er >> LV, er & (VEC - 1))]);
                 if (scl) {
                     C *cv = reinterpret_cast<C *>(&v);
 #pragma unroll
