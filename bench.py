@@ -413,7 +413,7 @@ def run_ours(args, rank: int, world: int):
     F = main["field_bytes"]
     peak, peak_kind = read_peaks()
     # dominant kernel: the three-stage fused line pass of the forward transform (2 launches
-    # per forward call: x pass persistent, y pass one line per CTA)
+    # per forward call: x pass persistent, y pass on buddy-line CTA pairs)
     t_launch = main["stage_ms"]["fwd"] / 2
     achieved = (2 * F) / (t_launch * 1e-3) / 1e9
     traffic, traffic_src = read_traffic("k3_pass_fwd_c64_N16384")
@@ -438,7 +438,7 @@ def run_ours(args, rank: int, world: int):
         "config": {"workload": WORKLOAD, "n": N, "p": P, "b": B, "dtype": "c64 (compensated FP32 twiddles)",
                    "l2": "inputs larger than L2 (2 GiB field per buffer)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
-        "roofline": {"bound": "hbm", "kernel": "k3_pass_kernel<6,8,fwd> (x pass persistent, y pass one line per CTA)",
+        "roofline": {"bound": "hbm", "kernel": "k3_pass_kernel<6,8,fwd> (x pass persistent, y pass on buddy-line CTA pairs)",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "traffic": traffic, "traffic_source": f"committed ncu capture ({traffic_src})",
