@@ -813,9 +813,13 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
         fwd_columns(hook);
         hook(3);
     } else if constexpr (!INV) {
-        // ================= forward, one row stage (RA2 == 1): one tile per cluster
-        // ---- 1. vector side -> local rows X (16-byte vectors, all loads before stores)
-        {
+        // ================= forward, one row stage (RA2 == 1): one tile per cluster.  With a
+        // contiguous vector side each thread reads its rows straight from global memory (two
+        // or more 16-byte loads per row, lanes on consecutive rows: a warp covers one run);
+        // otherwise the side moves through the rows X as 16-byte vectors first.
+        const bool rows_direct = (RA1 * sizeof(C)) % 16 == 0 && apos == 1;   // block-uniform
+        if (!rows_direct) {
+            // ---- 1. vector side -> local rows X (16-byte vectors, all loads before stores)
             uint4 buf[VPT];
 #pragma unroll
             for (int i = 0; i < VPT; i++) buf[i] = ldg16(in + aaddr((tid + i * NT) * VE));
@@ -834,21 +838,40 @@ __global__ void __launch_bounds__(NT, (fused_min_blocks<T, LV, LM, CL, TL, NT, I
                 const int u = tid + i * NT;
                 un1[i] = u % ML;
                 ut[i] = u / ML;
-                if constexpr ((RA1 * sizeof(C)) % 16 == 0 && (SG::XR * sizeof(C)) % 16 == 0) {
-                    // the row as 16-byte vectors: lanes on consecutive rows of XR = VEC + 2
-                    // points take distinct bank groups (8-byte reads of the same rows collide)
-                    const uint4 *rp = reinterpret_cast<const uint4 *>(&S[SG::X(ut[i], un1[i], 0)]);
+            }
+            if (rows_direct) {
+                if constexpr ((RA1 * sizeof(C)) % 16 == 0) {
+                    uint4 buf[NU][RA1 * sizeof(C) / 16];
 #pragma unroll
-                    for (int q = 0; q < RA1 * (int)sizeof(C) / 16; q++)
-                        *reinterpret_cast<uint4 *>(&v[i][q * 16 / (int)sizeof(C)]) = rp[q];
-                } else {
+                    for (int i = 0; i < NU; i++) {
+                        const uint4 *rp = reinterpret_cast<const uint4 *>(in + arow(ut[i], un1[i]));
 #pragma unroll
-                    for (int r = 0; r < RA1; r++) v[i][r] = S[SG::X(ut[i], un1[i], r)];
+                        for (int q = 0; q < RA1 * (int)sizeof(C) / 16; q++) buf[i][q] = __ldg(rp + q);
+                    }
+#pragma unroll
+                    for (int i = 0; i < NU; i++) memcpy(&v[i][0], &buf[i][0], RA1 * sizeof(C));
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < NU; i++) {
+                    if constexpr ((RA1 * sizeof(C)) % 16 == 0 && (SG::XR * sizeof(C)) % 16 == 0) {
+                        // the row as 16-byte vectors: lanes on consecutive rows of XR = VEC + 2
+                        // points take distinct bank groups (8-byte reads of the same rows collide)
+                        const uint4 *rp = reinterpret_cast<const uint4 *>(&S[SG::X(ut[i], un1[i], 0)]);
+#pragma unroll
+                        for (int q = 0; q < RA1 * (int)sizeof(C) / 16; q++)
+                            *reinterpret_cast<uint4 *>(&v[i][q * 16 / (int)sizeof(C)]) = rp[q];
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < RA1; r++) v[i][r] = S[SG::X(ut[i], un1[i], r)];
+                    }
                 }
             }
 #pragma unroll
             for (int i = 0; i < NU; i++) dft<RA1, DIR, T>(v[i]);
-            tile_sync<CL>();   // every CTA has finished reading its rows
+            // every CTA has finished reading its rows (the scatter overwrites them); with the
+            // rows read from global memory only a cluster needs it (its CTAs must have started)
+            if (!rows_direct || CL > 1) tile_sync<CL>();
 #pragma unroll
             for (int i = 0; i < NU; i++)
 #pragma unroll
