@@ -104,6 +104,44 @@ ZM_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memor
 ZM_DEV void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 ZM_DEV void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }   // all but the newest group
 
+// ------------------------------------------------ tensor memory (TMEM) staging
+// 128 lanes x 512 columns of 32 bits per SM.  With the 32x32b shape, warp w reaches the
+// 32 lanes 32 (w % 4) .. 32 (w % 4) + 31, lane i of the warp its own lane; an address is
+// (lane << 16) | column.  Every access is warp-wide (.sync.aligned).
+ZM_DEV void tmem_alloc(uint32_t *s_addr, unsigned ncols) {   // one warp
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(s_addr)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+ZM_DEV void tmem_dealloc(uint32_t taddr, unsigned ncols) {   // the allocating warp
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+ZM_DEV void tmem_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+ZM_DEV void tmem_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// 16 words of this thread to columns [c, c + 16) of its lane
+ZM_DEV void tmem_st16(uint32_t taddr, const uint32_t *w) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16};" ::"r"(taddr),
+        "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7]), "r"(w[8]), "r"(w[9]),
+        "r"(w[10]), "r"(w[11]), "r"(w[12]), "r"(w[13]), "r"(w[14]), "r"(w[15])
+        : "memory");
+}
+// waits for this thread's earlier TMEM stores, reads 16 words and waits for the read (in
+// one statement, so that no use of w can be scheduled before the data is there)
+ZM_DEV void tmem_ld16(uint32_t taddr, uint32_t *w) {
+    asm volatile(
+        "tcgen05.wait::st.sync.aligned;\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7]), "=r"(w[8]),
+          "=r"(w[9]), "=r"(w[10]), "=r"(w[11]), "=r"(w[12]), "=r"(w[13]), "=r"(w[14]), "=r"(w[15])
+        : "r"(taddr)
+        : "memory");
+}
+
 // ----------------------------------------------------- radix-R DFT codelets
 // Constant twiddles w_R^k = exp(DIR * 2 pi i k / R), DIR = -1 forward, +1 inverse.
 // cos(2 pi j / 32) for j = 0..8, the first octant of the 32-point circle.
