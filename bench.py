@@ -537,6 +537,15 @@ def run_profile_case(args):
         print(json.dumps({"profile_case": {"n": n, "p": P, "b": B, "dtype": args.profile_dtype,
                                            "ops": "inv", "field_bytes": pl.field_bytes}}))
         return
+    if args.profile_ops == "stencils":
+        # the three 2D stencils in one launch (Laplacian, dx, dy): four buffers
+        lap, gx, gy = pl.empty(), pl.empty(), pl.empty()
+        for _ in range(2):
+            pl.laplace_dx_dy(u, lap, gx, gy, inv_h2=float(n * n), delta=1.0 / n)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": {"n": n, "p": P, "b": B, "dtype": args.profile_dtype,
+                                           "ops": "stencils", "field_bytes": pl.field_bytes}}))
+        return
     if args.profile_ops == "fwd":
         # forward transform only (with a workspace, as in the timed step): three buffers
         spec, work = pl.empty(), pl.empty()
@@ -568,7 +577,7 @@ def main():
                     help="run the small profiling case only (for ncu captures)")
     ap.add_argument("--profile-n", type=int, default=8192)
     ap.add_argument("--profile-dtype", default="c64")
-    ap.add_argument("--profile-ops", choices=["all", "fwd", "inv", "lap3d", "fft3d", "batch", "layout"],
+    ap.add_argument("--profile-ops", choices=["all", "fwd", "inv", "stencils", "lap3d", "fft3d", "batch", "layout"],
                     default="all")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -810,9 +810,7 @@ static cudaError_t launch_s(const zm_plan_s *p, int op, const void *in, void *ou
     const S rd = (S)(1.0 / (12.0 * dl));
     if (p->g.dim == 2) {
         if (sizeof(S) == 4 && p->g.b % 4 == 0) {
-            // four rows of a B-row block per thread (FP32; the FP64 form stays one row
-            // per thread: its four-row form was slower, 4.20 -> 4.34 ms at N = 16384 for
-            // the three stencils in one launch)
+            // four rows of a B-row block per thread (FP32)
             const int64_t nt = nvec / 4;
             const unsigned g4 = (unsigned)((nt + threads - 1) / threads);
             if (op == ST_LAPLACE)
@@ -823,6 +821,19 @@ static cudaError_t launch_s(const zm_plan_s *p, int op, const void *in, void *ou
                 stencil_rows_kernel<S, NC, ST_DY, 4><<<g4, threads, 0, st>>>(i, o, o2, o3, p->g, nt, c, c2, rd);
             else
                 stencil_rows_kernel<S, NC, ST_ALL, 4><<<g4, threads, 0, st>>>(i, o, o2, o3, p->g, nt, c, c2, rd);
+        } else if (sizeof(S) == 8) {
+            // FP64: one row per thread, rows of the same B-row block addressed directly
+            // (two rows per thread, 70 registers, were slower: 4.20 -> 4.54 ms at N = 16384
+            // for the three stencils in one launch; four rows 4.34 ms)
+            const unsigned g1 = (unsigned)((nvec + threads - 1) / threads);
+            if (op == ST_LAPLACE)
+                stencil_rows_kernel<S, NC, ST_LAPLACE, 1><<<g1, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
+            else if (op == ST_DX)
+                stencil_rows_kernel<S, NC, ST_DX, 1><<<g1, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
+            else if (op == ST_DY)
+                stencil_rows_kernel<S, NC, ST_DY, 1><<<g1, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
+            else
+                stencil_rows_kernel<S, NC, ST_ALL, 1><<<g1, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
         } else if (op == ST_LAPLACE)
             stencil_kernel<S, NC, ST_LAPLACE, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
         else if (op == ST_DX)
