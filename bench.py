@@ -499,7 +499,8 @@ def run_profile_case(args):
                                            "elems": bt.total}}))
         return
     if args.profile_ops == "layout":
-        # natural -> interleaved converter and a reciprocal-space pointwise operator, N = 8192
+        # natural -> interleaved converter, a reciprocal-space pointwise operator and the
+        # natural <-> reciprocal converters, N = 8192
         n = args.profile_n
         pl = Plan(2, n, B, P, dtype=args.profile_dtype)
         nat, buf = pl.empty(), pl.empty()
@@ -507,6 +508,8 @@ def run_profile_case(args):
         for _ in range(2):
             pl.natural_to_real(nat, buf)
             pl.spectral_apply(buf, abi.ZM_SPECTRAL_GAUSSIAN, n / 16)
+            pl.natural_to_reciprocal(nat, buf)
+            pl.reciprocal_to_natural(buf, nat)
         torch.cuda.synchronize()
         print(json.dumps({"profile_case": {"n": n, "p": P, "b": B, "dtype": args.profile_dtype,
                                            "ops": "layout", "field_bytes": pl.field_bytes}}))

@@ -244,10 +244,8 @@ __global__ void __launch_bounds__(256) stencil_kernel(const S *__restrict__ in, 
 // (above a block's first row group, below its last) go through the block-cyclic maps as
 // in stencil_kernel; every output is computed by the same expressions, in the same order.
 template <typename S, int NC, int OP, int RY>
-__global__ void __launch_bounds__(256) stencil_rows_kernel(const S *__restrict__ in, S *__restrict__ out,
-                                                           S *__restrict__ out2, S *__restrict__ out3,
-                                                           const Geom g, int64_t nthreads, S coef, S coef2,
-                                                           S rden) {
+ZM_DEV void stencil_rows_body(const S *__restrict__ in, S *__restrict__ out, S *__restrict__ out2,
+                              S *__restrict__ out3, const Geom &g, int64_t nthreads, S coef, S coef2, S rden) {
     using O = ops<S>;
     using V = vec16<S>;
     constexpr int K = V::n / NC;                 // elements per vector
@@ -381,6 +379,25 @@ __global__ void __launch_bounds__(256) stencil_rows_kernel(const S *__restrict__
         *reinterpret_cast<uint4 *>(out2 + e * NC) = *reinterpret_cast<const uint4 *>(&rx);
         *reinterpret_cast<uint4 *>(out3 + e * NC) = *reinterpret_cast<const uint4 *>(&ry);
     }
+}
+
+// The kernels: the default register allocation (four rows per thread, FP32), and one
+// row per thread in FP64 held to 51 registers, five CTAs per SM (the FP64 kernel waits on
+// its loads: 56 registers and four CTAs per SM left the three stencils at 4.01 ms at
+// N = 16384 c128, five take 3.72 ms)
+template <typename S, int NC, int OP, int RY>
+__global__ void __launch_bounds__(256) stencil_rows_kernel(const S *__restrict__ in, S *__restrict__ out,
+                                                           S *__restrict__ out2, S *__restrict__ out3,
+                                                           const Geom g, int64_t nthreads, S coef, S coef2,
+                                                           S rden) {
+    stencil_rows_body<S, NC, OP, RY>(in, out, out2, out3, g, nthreads, coef, coef2, rden);
+}
+template <typename S, int NC, int OP>
+__global__ void __launch_bounds__(256, 5) stencil_rows1_kernel(const S *__restrict__ in, S *__restrict__ out,
+                                                               S *__restrict__ out2, S *__restrict__ out3,
+                                                               const Geom g, int64_t nthreads, S coef, S coef2,
+                                                               S rden) {
+    stencil_rows_body<S, NC, OP, 1>(in, out, out2, out3, g, nthreads, coef, coef2, rden);
 }
 
 // 3D Laplacian (laplace3d.cu:98-224 accumulation order) with RX vectors of one line per
@@ -822,18 +839,18 @@ static cudaError_t launch_s(const zm_plan_s *p, int op, const void *in, void *ou
             else
                 stencil_rows_kernel<S, NC, ST_ALL, 4><<<g4, threads, 0, st>>>(i, o, o2, o3, p->g, nt, c, c2, rd);
         } else if (sizeof(S) == 8) {
-            // FP64: one row per thread, rows of the same B-row block addressed directly
-            // (two rows per thread, 70 registers, were slower: 4.20 -> 4.54 ms at N = 16384
-            // for the three stencils in one launch; four rows 4.34 ms)
+            // FP64: one row per thread, rows of the same B-row block addressed directly, five
+            // CTAs per SM (two rows per thread, 70 registers, were slower: 4.20 -> 4.54 ms at
+            // N = 16384 for the three stencils in one launch; four rows 4.34 ms)
             const unsigned g1 = (unsigned)((nvec + threads - 1) / threads);
             if (op == ST_LAPLACE)
-                stencil_rows_kernel<S, NC, ST_LAPLACE, 1><<<g1, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
+                stencil_rows1_kernel<S, NC, ST_LAPLACE><<<g1, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
             else if (op == ST_DX)
-                stencil_rows_kernel<S, NC, ST_DX, 1><<<g1, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
+                stencil_rows1_kernel<S, NC, ST_DX><<<g1, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
             else if (op == ST_DY)
-                stencil_rows_kernel<S, NC, ST_DY, 1><<<g1, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
+                stencil_rows1_kernel<S, NC, ST_DY><<<g1, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
             else
-                stencil_rows_kernel<S, NC, ST_ALL, 1><<<g1, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
+                stencil_rows1_kernel<S, NC, ST_ALL><<<g1, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
         } else if (op == ST_LAPLACE)
             stencil_kernel<S, NC, ST_LAPLACE, 2><<<grid, threads, 0, st>>>(i, o, o2, o3, p->g, nvec, c, c2, rd);
         else if (op == ST_DX)

@@ -56,7 +56,10 @@ def test_adjoint_dot_products(dim, n, b, p, dt):
 
 
 @pytest.mark.parametrize("dt", ["c128", "c64"])
-@pytest.mark.parametrize("dim,n,b,p", [(2, 64, 4, 2), (2, 128, 8, 4), (3, 16, 2, 2), (3, 32, 2, 4)])
+@pytest.mark.parametrize("dim,n,b,p", [(2, 64, 4, 2), (2, 128, 8, 4), (3, 16, 2, 2), (3, 32, 2, 4),
+                                       # the tiled reciprocal converter: runs of 4, 8, 16, 32
+                                       (2, 4096, 64, 4), (2, 1024, 32, 2), (2, 2048, 32, 2),
+                                       (2, 2048, 16, 2), (3, 256, 8, 2)])
 def test_layout_converters(dim, n, b, p, dt):
     import torch
     pl = _plan(dim, n, b, p, dt)
