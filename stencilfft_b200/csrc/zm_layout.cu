@@ -58,8 +58,7 @@ __global__ void __launch_bounds__(256) convert_kernel(const cpx<T> *__restrict__
 // the transpose of a natural block made of TB runs of TB contiguous elements.  A CTA
 // takes SB = 1024 / TB^2 blocks side by side along the positions (TB rows x SB TB
 // positions, 1024 elements): it moves the natural side as runs of TB elements and the
-// reciprocal side as runs of SB TB, both four elements per thread, through a padded
-// shared-memory tile.  (The element-wise kernel gathered or scattered one element per
+// reciprocal side as runs of SB TB through a padded shared-memory tile.  (The element-wise kernel gathered or scattered one element per
 // natural row: 38 % of the copy bandwidth for natural -> reciprocal at N = 8192 c64.)
 template <typename T, int TB, bool TO_NAT>
 __global__ void __launch_bounds__(256) recip_tile_kernel(const cpx<T> *__restrict__ in, cpx<T> *__restrict__ out,
@@ -99,29 +98,42 @@ __global__ void __launch_bounds__(256) recip_tile_kernel(const cpx<T> *__restric
         return (kpos * spos) + kmid * g.n + k2base + j;
     };
     auto tidx = [](int b, int i, int j) { return (b * TB + i) * (TB + 1) + j; };
+    // element x = tid + 256 u of the CTA on both sides: consecutive lanes take consecutive
+    // elements of a run, so the shared tile (rows of TB + 1) is read and written without
+    // bank conflicts on either side and every warp access covers whole runs
     if (!TO_NAT) {
         cpx<T> v[4];
-        const int64_t a = nat_addr(4 * tid);
-        ld_run(in + a, v);
-        const int x = 4 * tid, b = x / (TB * TB), i = (x / TB) % TB, j = x % TB;
 #pragma unroll
-        for (int u = 0; u < 4; u++) tile[tidx(b, i, j + u)] = v[u];
+        for (int u = 0; u < 4; u++) v[u] = ldg(in + nat_addr(tid + 256 * u));
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int x = tid + 256 * u;
+            tile[tidx(x / (TB * TB), (x / TB) % TB, x % TB)] = v[u];
+        }
         __syncthreads();
-        const int jr = x / W, pr = x % W;
 #pragma unroll
-        for (int u = 0; u < 4; u++) v[u] = tile[tidx((pr + u) / TB, (pr + u) % TB, jr)];
-        st_run(out + rbase + (int64_t)jr * L + pr, v);
+        for (int u = 0; u < 4; u++) {
+            const int x = tid + 256 * u, jr = x / W, pr = x % W;
+            out[rbase + (int64_t)jr * L + pr] = tile[tidx(pr / TB, pr % TB, jr)];
+        }
     } else {
         cpx<T> v[4];
-        const int x = 4 * tid, jr = x / W, pr = x % W;
-        ld_run(in + rbase + (int64_t)jr * L + pr, v);
 #pragma unroll
-        for (int u = 0; u < 4; u++) tile[tidx((pr + u) / TB, (pr + u) % TB, jr)] = v[u];
+        for (int u = 0; u < 4; u++) {
+            const int x = tid + 256 * u, jr = x / W, pr = x % W;
+            v[u] = ldg(in + rbase + (int64_t)jr * L + pr);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int x = tid + 256 * u, jr = x / W, pr = x % W;
+            tile[tidx(pr / TB, pr % TB, jr)] = v[u];
+        }
         __syncthreads();
-        const int b = x / (TB * TB), i = (x / TB) % TB, j = x % TB;
 #pragma unroll
-        for (int u = 0; u < 4; u++) v[u] = tile[tidx(b, i, j + u)];
-        st_run(out + nat_addr(x), v);
+        for (int u = 0; u < 4; u++) {
+            const int x = tid + 256 * u;
+            out[nat_addr(x)] = tile[tidx(x / (TB * TB), (x / TB) % TB, x % TB)];
+        }
     }
 }
 
@@ -184,10 +196,18 @@ __global__ void __launch_bounds__(256) spectral_kernel(cpx<T> *__restrict__ d, c
     ld_run(d + e0, v);
     const int64_t half = g.n >> 1;
     const T inv2a2 = (T)(1.0 / (2.0 * a * a)), inva2 = (T)(1.0 / (a * a)), ta = (T)a;
+    // the CEPT elements are consecutive positions of one row; inside a run of VP positions
+    // the position axis' frequency (k1 in 2D, k0 in 3D) steps by one and the others stay
+    int64_t k0, k1, k2;
+    recip_k(e0, g, k0, k1, k2);
+    const bool run = g.vp >= CEPT;
 #pragma unroll
     for (int i = 0; i < CEPT; i++) {
-        int64_t k0, k1, k2;
-        recip_k(e0 + i, g, k0, k1, k2);
+        if (i > 0) {
+            if (!run) recip_k(e0 + i, g, k0, k1, k2);
+            else if (g.dim == 2) k1++;
+            else k0++;
+        }
         const int64_t s0 = k0 >= half ? k0 - g.n : k0;
         const int64_t s1 = k1 >= half ? k1 - g.n : k1;
         const int64_t s2 = k2 >= half ? k2 - g.n : k2;
