@@ -336,20 +336,20 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batch_kernel(const BatchPara
             __syncthreads();
             const cpx<T> *in = reinterpret_cast<const cpx<T> *>(S.in) + sf.off;
             cpx<T> *out = reinterpret_cast<cpx<T> *>(S.out) + sf.off;
-            // SwzV4<S>: S = 2 + log2 of the first column stage's radix (radix_sched)
-#define ZM_BT(LMC, SS) batch_tile<T, EPT, LMC, SwzV4<SS>>(S.op, S.scale != 0, S.a, sf, c, s, in, out, l0, nthr, tid)
+            // slot permutation per column length (SwzX, zm_tile.cuh)
+#define ZM_BT(LMC, ...) batch_tile<T, EPT, LMC, __VA_ARGS__>(S.op, S.scale != 0, S.a, sf, c, s, in, out, l0, nthr, tid)
             bool done = false;
             if constexpr (sizeof(T) == 4 && EPT == 16) {
                 if (g.logVEC == 2) {
                     done = true;
                     switch (g.logM) {
-                    case 4: ZM_BT(4, 6); break;
-                    case 5: ZM_BT(5, 6); break;
-                    case 6: ZM_BT(6, 4); break;
-                    case 7: ZM_BT(7, 5); break;
-                    case 8: ZM_BT(8, 6); break;
-                    case 9: ZM_BT(9, 3); break;
-                    case 10: ZM_BT(10, 4); break;
+                    case 4: ZM_BT(4, SwzX<4, 8, 4, 6, 0>); break;
+                    case 5: ZM_BT(5, SwzX<3, 9, 7, 4, 6>); break;
+                    case 6: ZM_BT(6, SwzX<3, 8, 0, 4, 10>); break;
+                    case 7: ZM_BT(7, SwzX<3, 4, 10, 5, 8>); break;
+                    case 8: ZM_BT(8, SwzX<4, 9, 4, 6, 10>); break;
+                    case 9: ZM_BT(9, SwzX<3, 10, 0, 4, 6>); break;
+                    case 10: ZM_BT(10, SwzX<3, 0, 0, 4, 0>); break;
                     default: done = false; break;
                     }
                 }

@@ -14,17 +14,23 @@
 namespace zm {
 
 // Physical slot of tile element i in shared memory.  SwzNone: the element itself.
-// SwzV4<S> (tiles with VEC = 4): i ^ (i >> 4 & 3) ^ ((i >> S & 3) << 2), a permutation
-// inside every aligned run of 16 elements, chosen so that the 16 lanes of a half-warp
-// hit 16 distinct bank pairs in every stage: the row stage (lanes on rows 4 elements
-// apart), the first column stage's Stockham writes (lanes on units 4 R elements apart,
-// S = 2 + log2 R) and contiguous runs (unchanged).  Without it those accesses were 4-way
-// conflicted.
+// SwzX (tiles with VEC = 4): up to five two-bit fields of i (shift 0 = no field) XORed
+// into bits 0-1 (A0, A1), 1-2 (B) and 2-3 (C0, C1), a permutation inside every aligned run
+// of 16 elements that is linear over XOR (SwzX::f(a ^ c) = SwzX::f(a) ^ SwzX::f(c)).  The
+// shifts per column length M are the ones a bank-conflict model of every shared access of
+// a tile found conflict-free for 16-lane half-warps: the row sweeps (lanes on rows 4
+// elements apart), each Stockham stage's reads and writes, and both frequency-side
+// sweeps (x pass: lines fastest, a stride of N elements; y pass: runs of VP = 2).  The
+// earlier two-field form, tuned on the stages alone, left the x pass's frequency sweep
+// 2- to 16-way conflicted.
 struct SwzNone {
-    static ZM_DEV int f(int i) { return i; }
+    static constexpr ZM_DEV int f(int i) { return i; }
 };
-template <int S> struct SwzV4 {
-    static ZM_DEV int f(int i) { return i ^ ((i >> 4) & 3) ^ (((i >> S) & 3) << 2); }
+template <int A0, int A1, int B, int C0, int C1> struct SwzX {
+    template <int S, int T> static constexpr ZM_DEV int fld(int i) { return S ? ((i >> S) & 3) << T : 0; }
+    static constexpr ZM_DEV int f(int i) {
+        return i ^ fld<A0, 0>(i) ^ fld<A1, 0>(i) ^ fld<B, 1>(i) ^ fld<C0, 2>(i) ^ fld<C1, 2>(i);
+    }
 };
 
 // ------------------------------------------------------------ Stockham stage
@@ -165,10 +171,14 @@ ZM_DEV void stockham_stage_ct(cpx<T> *s, int tid, const tw<T> *twN) {
         }
         base[u] = bb;
         jv[u] = j;
+        // bb, j str and r nR str occupy disjoint bits and the slot permutations are linear
+        // over XOR: SW::f(bb + i str) = SW::f(bb + j str) ^ SW::f(r nR str), one XOR with a
+        // constant per access
+        const int fa = SW::f(bb + j * str);
 #pragma unroll
         for (int r = 0; r < R; r++) {
             const int i = j + r * nR;
-            cpx<T> x = s[SW::f(bb + i * str)];
+            cpx<T> x = s[fa ^ SW::f(r * nR * str)];
             if constexpr (PRETW) x = twmul<CONJ>(x, ldtw(twN, (int64_t)i * tagn));
             v[u][r] = x;
         }
@@ -184,9 +194,10 @@ ZM_DEV void stockham_stage_ct(cpx<T> *s, int tid, const tw<T> *twN) {
             for (int r = 1; r < R; r++) v[u][r] = twmul<CONJ>(v[u][r], ldtw(twN, ((int64_t)k * r) << sh));
         }
         dft<R, DIR, T>(v[u]);
-        const int idxD = (j - k) * R + k;
+        const int idxD = (j - k) * R + k;   // (j - k) R and k leave the bits of r NS free
+        const int fw = SW::f(base[u] + idxD * str);
 #pragma unroll
-        for (int r = 0; r < R; r++) s[SW::f(base[u] + (idxD + r * NS) * str)] = v[u][r];
+        for (int r = 0; r < R; r++) s[fw ^ SW::f(r * NS * str)] = v[u][r];
     }
     __syncthreads();
 }
@@ -368,9 +379,9 @@ ZM_DEV void tile_load_rows_v4(const Tile &c, const Geom &g, cpx<float> *s, const
         cpx<float> x[4] = {{v[q][0].x, v[q][0].y}, {v[q][0].z, v[q][0].w}, {v[q][1].x, v[q][1].y},
                            {v[q][1].z, v[q][1].w}};
         dft<4, -1, float>(x);
-        const int rho = tid + q * NT;
+        const int f0 = SW::f((tid + q * NT) * 4);   // the slot permutations leave bits 0-1 to k
 #pragma unroll
-        for (int k = 0; k < 4; k++) s[SW::f(rho * 4 + k)] = x[k];
+        for (int k = 0; k < 4; k++) s[f0 ^ k] = x[k];
     }
 }
 template <int EPT, int LM, int NT, typename SW>
@@ -382,8 +393,9 @@ ZM_DEV void tile_rows_store_v4(const Tile &c, const Geom &g, const cpx<float> *s
         const int rho = tid + q * NT;
         const int n1 = rho & (M - 1);
         cpx<float> x[4];
+        const int f0 = SW::f(rho * 4);
 #pragma unroll
-        for (int k = 0; k < 4; k++) x[k] = twmul<true>(s[SW::f(rho * 4 + k)], ldtw(twN, (int64_t)k * n1));
+        for (int k = 0; k < 4; k++) x[k] = twmul<true>(s[f0 ^ k], ldtw(twN, (int64_t)k * n1));
         dft<4, 1, float>(x);
         if (scl)
 #pragma unroll
