@@ -136,9 +136,9 @@ ZM_DEV int64_t real_elem(int64_t gr, int64_t gc, const Geom &g) {
 }
 
 // Both sub-transforms of a tile: compile-time-sized stages (LMC = log2 M) for the
-// complex64 tiles with VEC = 4 (the layout the B autotuner picks for the batch sizes, B =
-// N / 8 at P = 2), or the runtime-sized stages (LMC = 0) for every other shape.
-// (LMC > 0: the column sub-transform only; the row stage runs fused with the
+// complex64 tiles with VEC = 4 and P = 2 or 4 (the layout the B autotuner picks for the
+// batch sizes, B = N / 8 at P = 2), or the runtime-sized stages (LMC = 0) for every other
+// shape.  (LMC > 0: the column sub-transform only; the row stage runs fused with the
 // vector-side sweep, tile_load_rows_v4 / tile_rows_store_v4)
 template <typename T, int EPT, bool INV, int LM, typename SW>
 __device__ __noinline__ void tile_transform_v4(cpx<T> *s, int tid, const tw<T> *twN) {
@@ -156,28 +156,53 @@ ZM_DEV void batch_tile_transform(cpx<T> *s, const BatchField &f, int nthr, int t
 
 // One tile of an axis-pass step: load, transform(s), store.  SW is the shared-memory
 // slot permutation of the tile (SwzV4 for the compile-time VEC = 4 tiles).
-template <typename T, int EPT, int LMC, typename SW>
+template <typename T, int EPT, int LMC, typename SW, int LP = 0>
 __device__ __noinline__ void batch_tile(int op, bool scale, double a, const BatchField &sf, const Tile c, cpx<T> *s,
                                         const cpx<T> *in, cpx<T> *out, int64_t l0, int nthr, int tid) {
     const Geom &g = sf.g;
     const tw<T> *twN = reinterpret_cast<const tw<T> *>(sf.twN);
     const bool xpass = op == BOP_X_FWD || op == BOP_X_INV;
-    // vector-side sweeps: plain, or with the VEC = 4 row stage fused in (LMC > 0)
+    // vector-side sweeps: plain, or with the VEC = 4 row stage fused in and every size
+    // fixed (LMC > 0, P = 2^LP); likewise the frequency-side sweeps
     auto load_vec = [&]() {
-        if constexpr (LMC > 0) tile_load_rows_v4<EPT, LMC, kBatchThreads, SW>(c, g, s, in, tid);
-        else tile_load_vec<EPT, SW>(c, g, s, in, nthr, tid);
+        if constexpr (LMC > 0) {
+            if (xpass) tile_load_rows_v4<EPT, LMC, LP, true, kBatchThreads, SW>(c, s, in, tid);
+            else tile_load_rows_v4<EPT, LMC, LP, false, kBatchThreads, SW>(c, s, in, tid);
+        } else {
+            tile_load_vec<EPT, SW>(c, g, s, in, nthr, tid);
+        }
     };
     auto store_vec = [&](bool scl, T sc) {
-        if constexpr (LMC > 0) tile_rows_store_v4<EPT, LMC, kBatchThreads, SW>(c, g, s, out, scl, sc, (T)0, twN, tid);
-        else tile_store_vec<EPT, SW>(c, g, s, out, scl, sc, (T)0, nthr, tid);
+        if constexpr (LMC > 0) {
+            if (xpass) tile_rows_store_v4<EPT, LMC, LP, true, kBatchThreads, SW>(c, s, out, scl, sc, (T)0, twN, tid);
+            else tile_rows_store_v4<EPT, LMC, LP, false, kBatchThreads, SW>(c, s, out, scl, sc, (T)0, twN, tid);
+        } else {
+            tile_store_vec<EPT, SW>(c, g, s, out, scl, sc, (T)0, nthr, tid);
+        }
+    };
+    auto store_freq = [&]() {
+        if constexpr (LMC > 0) {
+            if (xpass) tile_freq_v4<EPT, LMC, LP, true, kBatchThreads, false, SW>(c, s, in, out, tid);
+            else tile_freq_v4<EPT, LMC, LP, false, kBatchThreads, false, SW>(c, s, in, out, tid);
+        } else {
+            tile_store_freq<EPT, SW>(c, g, s, out, false, (T)1, (T)0, nthr, tid);
+        }
+    };
+    auto load_freq = [&]() {
+        if constexpr (LMC > 0) {
+            if (xpass) tile_freq_v4<EPT, LMC, LP, true, kBatchThreads, true, SW>(c, s, in, out, tid);
+            else tile_freq_v4<EPT, LMC, LP, false, kBatchThreads, true, SW>(c, s, in, out, tid);
+        } else {
+            tile_load_freq<EPT, SW>(c, g, s, in, nthr, tid);
+        }
     };
     if (op == BOP_X_FWD || op == BOP_Y_FWD) {
         load_vec();
         __syncthreads();
         batch_tile_transform<T, EPT, false, LMC, SW>(s, sf, nthr, tid, twN);
-        tile_store_freq<EPT, SW>(c, g, s, out, false, (T)1, (T)0, nthr, tid);
+        store_freq();
     } else if (op == BOP_X_INV || op == BOP_Y_INV) {
-        tile_load_freq<EPT, SW>(c, g, s, in, nthr, tid);
+        load_freq();
         __syncthreads();
         batch_tile_transform<T, EPT, true, LMC, SW>(s, sf, nthr, tid, twN);
         const bool scl = scale && xpass;
@@ -337,10 +362,12 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batch_kernel(const BatchPara
             const cpx<T> *in = reinterpret_cast<const cpx<T> *>(S.in) + sf.off;
             cpx<T> *out = reinterpret_cast<cpx<T> *>(S.out) + sf.off;
             // slot permutation per column length (SwzX, zm_tile.cuh)
-#define ZM_BT(LMC, ...) batch_tile<T, EPT, LMC, __VA_ARGS__>(S.op, S.scale != 0, S.a, sf, c, s, in, out, l0, nthr, tid)
+#define ZM_BT(LMC, ...)                                                                                \
+    (g.logP == 1 ? batch_tile<T, EPT, LMC, __VA_ARGS__, 1>(S.op, S.scale != 0, S.a, sf, c, s, in, out, l0, nthr, tid) \
+                 : batch_tile<T, EPT, LMC, __VA_ARGS__, 2>(S.op, S.scale != 0, S.a, sf, c, s, in, out, l0, nthr, tid))
             bool done = false;
             if constexpr (sizeof(T) == 4 && EPT == 16) {
-                if (g.logVEC == 2) {
+                if (g.logVEC == 2 && (g.logP == 1 || g.logP == 2)) {
                     done = true;
                     switch (g.logM) {
                     case 4: ZM_BT(4, SwzX<4, 8, 4, 6, 0>); break;

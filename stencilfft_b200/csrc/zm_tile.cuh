@@ -361,16 +361,30 @@ ZM_DEV void tile_store_vec(const Tile &c, const Geom &g, const cpx<T> *s, cpx<T>
 //            (k2 = 0 .. 3), the radix-4 DFT, the optional scale of tile_store_vec, two
 //            16-byte stores.
 // This drops one shared-memory round trip and its two barriers per tile.
-template <int EPT, int LM, int NT, typename SW>
-ZM_DEV void tile_load_rows_v4(const Tile &c, const Geom &g, cpx<float> *s, const cpx<float> *in, int tid) {
+//
+// These sweeps, and the frequency-side one below (tile_freq_v4), have every size fixed
+// at compile time: M = 2^LM, P = 2^LP and the pass (XP: the 2D x pass, vector side the
+// real layout's rows, frequency side a stride of L with the lines fastest; otherwise
+// the y pass, both sides runs of L).  Offsets inside one field (N^2 <= 2^24 elements)
+// are 32-bit.
+template <int LM, int LP, bool XP> struct V4Geom {
+    static constexpr int LN = LM + 2, N = 1 << LN, LL = LN - LP, L = 1 << LL, LVP = 2 - LP, VP = 1 << LVP;
+    static constexpr int CHUNK = XP ? L * L : (L * L) << LP;   // the next rank of a line (a_chunk, f_chunk)
+    static constexpr int FPOS = XP ? L : 1;                    // frequency-side position stride (f_pos)
+    static_assert(LP >= 0 && LP <= 2, "VEC = 4 needs P <= 4");
+};
+
+template <int EPT, int LM, int LP, bool XP, int NT, typename SW>
+ZM_DEV void tile_load_rows_v4(const Tile &c, cpx<float> *s, const cpx<float> *in, int tid) {
+    using G = V4Geom<LM, LP, XP>;
     constexpr int RPT = EPT / 4, M = 1 << LM;
     float4 v[RPT][2];
 #pragma unroll
     for (int q = 0; q < RPT; q++) {
         const int rho = tid + q * NT;
         const int t = rho >> LM, r = (rho & (M - 1)) << 2;
-        const int ch = r >> g.logL, pos = r & (int)(g.L - 1);
-        const float4 *p = reinterpret_cast<const float4 *>(in + c.abase[t] + ch * c.a_chunk + pos);
+        const int off = (int)c.abase[t] + (r >> G::LL) * G::CHUNK + (r & (G::L - 1));
+        const float4 *p = reinterpret_cast<const float4 *>(in + off);
         v[q][0] = __ldg(p);
         v[q][1] = __ldg(p + 1);
     }
@@ -384,9 +398,10 @@ ZM_DEV void tile_load_rows_v4(const Tile &c, const Geom &g, cpx<float> *s, const
         for (int k = 0; k < 4; k++) s[f0 ^ k] = x[k];
     }
 }
-template <int EPT, int LM, int NT, typename SW>
-ZM_DEV void tile_rows_store_v4(const Tile &c, const Geom &g, const cpx<float> *s, cpx<float> *out, bool scl,
-                               float sr, float si, const tw<float> *twN, int tid) {
+template <int EPT, int LM, int LP, bool XP, int NT, typename SW>
+ZM_DEV void tile_rows_store_v4(const Tile &c, const cpx<float> *s, cpx<float> *out, bool scl, float sr, float si,
+                               const tw<float> *twN, int tid) {
+    using G = V4Geom<LM, LP, XP>;
     constexpr int RPT = EPT / 4, M = 1 << LM;
 #pragma unroll
     for (int q = 0; q < RPT; q++) {
@@ -401,10 +416,49 @@ ZM_DEV void tile_rows_store_v4(const Tile &c, const Geom &g, const cpx<float> *s
 #pragma unroll
             for (int k = 0; k < 4; k++) x[k] = {sr * x[k].x - si * x[k].y, sr * x[k].y + si * x[k].x};
         const int t = rho >> LM, r = n1 << 2;
-        const int ch = r >> g.logL, pos = r & (int)(g.L - 1);
-        float4 *p = reinterpret_cast<float4 *>(out + c.abase[t] + ch * c.a_chunk + pos);
+        const int off = (int)c.abase[t] + (r >> G::LL) * G::CHUNK + (r & (G::L - 1));
+        float4 *p = reinterpret_cast<float4 *>(out + off);
         p[0] = make_float4(x[0].x, x[0].y, x[1].x, x[1].y);
         p[1] = make_float4(x[2].x, x[2].y, x[3].x, x[3].y);
+    }
+}
+
+// Frequency side <-> slots s[t][k1 VEC + c VP + f] (tile_load_freq / tile_store_freq):
+// element e = tid + i NT is (line t, chunk c, position pos = k1 VP + f), lines fastest on
+// the x pass's strided side.  LOAD: all EPT loads in flight, then the shared-memory writes.
+template <int EPT, int LM, int LP, bool XP, int NT, bool LOAD, typename SW>
+ZM_DEV void tile_freq_v4(const Tile &c, cpx<float> *s, const cpx<float> *in, cpx<float> *out, int tid) {
+    using G = V4Geom<LM, LP, XP>;
+    constexpr int TL = NT * EPT >> G::LN, LT = ct_log2(TL);
+    auto coords = [&](int i, int &slot, int &off) {
+        const int e = tid + i * NT;
+        const int t = XP ? (e & (TL - 1)) : (e >> G::LN);
+        const int cp = XP ? (e >> LT) : (e & (G::N - 1));
+        const int ch = cp >> G::LL, pos = cp & (G::L - 1);
+        slot = (t << G::LN) + ((pos >> G::LVP) << 2) + (ch << G::LVP) + (pos & (G::VP - 1));
+        off = (int)c.fbase[t] + ch * G::CHUNK + pos * G::FPOS;
+    };
+    if constexpr (LOAD) {
+        cpx<float> v[EPT];
+#pragma unroll
+        for (int i = 0; i < EPT; i++) {
+            int slot, off;
+            coords(i, slot, off);
+            v[i] = ldg(in + off);
+        }
+#pragma unroll
+        for (int i = 0; i < EPT; i++) {
+            int slot, off;
+            coords(i, slot, off);
+            s[SW::f(slot)] = v[i];
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < EPT; i++) {
+            int slot, off;
+            coords(i, slot, off);
+            out[off] = s[SW::f(slot)];
+        }
     }
 }
 
