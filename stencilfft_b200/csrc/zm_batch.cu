@@ -239,6 +239,93 @@ __device__ __noinline__ void batch_tile(int op, bool scale, double a, const Batc
     }
 }
 
+// One tile of the residual step, out = Lap_h(in) - rhs over elements [e0, e0 + TP) of a
+// field (5-point, periodic, h = length / N, a = 1 / length); its own function so that its
+// registers do not weigh on the rest of the persistent kernel.
+template <typename T, int TP>
+__device__ __noinline__ void residual_tile(const Geom &g, double a, const cpx<T> *in, const cpx<T> *rhs, cpx<T> *out,
+                                           int64_t e0, int nthr, int tid) {
+    const T inv_h2 = (T)((double)g.n * a * (double)g.n * a);
+    const int64_t m = g.n - 1;
+    auto resid = [&](const cpx<T> &up, const cpx<T> &dn, const cpx<T> &lf, const cpx<T> &rt,
+                     const cpx<T> &c, const cpx<T> &r) -> cpx<T> {
+        const T lx = up.x + dn.x + lf.x + rt.x - (T)4 * c.x;
+        const T ly = up.y + dn.y + lf.y + rt.y - (T)4 * c.y;
+        return {lx * inv_h2 - r.x, ly * inv_h2 - r.y};
+    };
+    if constexpr (sizeof(T) == 4) {
+        // Pairs (e, e + 1), e even: the two share rank and row (L is even), so
+        // their up / down neighbours are again two adjacent elements, and so
+        // are left / right except at a block edge.  Adjacent 16-byte-aligned
+        // pairs move as one 16-byte access, anything else element by element.
+        auto ld2 = [](const cpx<T> *p0, const cpx<T> *p1, cpx<T> &v0, cpx<T> &v1) {
+            if (p1 == p0 + 1 && ((uintptr_t)p0 & 15) == 0) {
+                const float4 q = __ldg(reinterpret_cast<const float4 *>(p0));
+                v0 = {q.x, q.y};
+                v1 = {q.z, q.w};
+            } else {
+                v0 = ldg(p0);
+                v1 = ldg(p1);
+            }
+        };
+        // Inside a rank's B x B block (in-block column j = pos >> log VEC and
+        // row lr mod B both off the block's edges) the four neighbours of the
+        // pair sit in the same rank at -L, +L (rows) and -VEC, +VEC (columns:
+        // the next global column is the next in-block column of the same
+        // block cycle), adjacent pairs again when VEC >= 2.
+        const bool fast = g.logVEC >= 1 &&
+                          (((uintptr_t)in | (uintptr_t)rhs | (uintptr_t)out) & 15) == 0;
+        const int iL = (int)g.L, iV = (int)g.vec, bm = (int)g.b - 1;
+        auto q4 = [](const cpx<T> *q) { return __ldg(reinterpret_cast<const float4 *>(q)); };
+        for (int i = tid; i < TP / 2; i += nthr) {
+            const int64_t e = e0 + 2 * i;
+            const int pos = (int)(e & (g.L - 1)), lr = (int)((e >> g.logL) & (g.L - 1));
+            const int j = pos >> g.logVEC, rb = lr & bm;
+            if (fast && j > 0 && j < bm && rb > 0 && rb < bm) {
+                const cpx<T> *pc = in + e;
+                const float4 up = q4(pc - iL), dn = q4(pc + iL), lf = q4(pc - iV), rt = q4(pc + iV);
+                const float4 cc = q4(pc), rr = q4(rhs + e);
+                const cpx<T> o0 = resid({up.x, up.y}, {dn.x, dn.y}, {lf.x, lf.y}, {rt.x, rt.y},
+                                        {cc.x, cc.y}, {rr.x, rr.y});
+                const cpx<T> o1 = resid({up.z, up.w}, {dn.z, dn.w}, {lf.z, lf.w}, {rt.z, rt.w},
+                                        {cc.z, cc.w}, {rr.z, rr.w});
+                *reinterpret_cast<float4 *>(out + e) = make_float4(o0.x, o0.y, o1.x, o1.y);
+                continue;
+            }
+            const int64_t gi0 = real_gidx(e, g), gc1 = real_gidx(e + 1, g) & m;
+            const int64_t gr = gi0 >> g.logN, gc0 = gi0 & m;
+            const int64_t au = real_elem((gr - 1) & m, gc0, g), ad = real_elem((gr + 1) & m, gc0, g);
+            cpx<T> up0, up1, dn0, dn1, lf0, lf1, rt0, rt1, c0, c1, r0, r1;
+            ld2(in + au, in + au + 1, up0, up1);
+            ld2(in + ad, in + ad + 1, dn0, dn1);
+            ld2(in + real_elem(gr, (gc0 - 1) & m, g), in + real_elem(gr, (gc1 - 1) & m, g), lf0, lf1);
+            ld2(in + real_elem(gr, (gc0 + 1) & m, g), in + real_elem(gr, (gc1 + 1) & m, g), rt0, rt1);
+            ld2(in + e, in + e + 1, c0, c1);
+            ld2(rhs + e, rhs + e + 1, r0, r1);
+            const cpx<T> o0 = resid(up0, dn0, lf0, rt0, c0, r0);
+            const cpx<T> o1 = resid(up1, dn1, lf1, rt1, c1, r1);
+            cpx<T> *po = out + e;
+            if (((uintptr_t)po & 15) == 0) {
+                *reinterpret_cast<float4 *>(po) = make_float4(o0.x, o0.y, o1.x, o1.y);
+            } else {
+                po[0] = o0;
+                po[1] = o1;
+            }
+        }
+    } else {
+        for (int i = tid; i < TP; i += nthr) {
+            const int64_t e = e0 + i;
+            const int64_t gi = real_gidx(e, g);
+            const int64_t gr = gi >> g.logN, gc = gi & m;
+            const cpx<T> up = ldg(in + real_elem((gr - 1) & m, gc, g));
+            const cpx<T> dn = ldg(in + real_elem((gr + 1) & m, gc, g));
+            const cpx<T> lf = ldg(in + real_elem(gr, (gc - 1) & m, g));
+            const cpx<T> rt = ldg(in + real_elem(gr, (gc + 1) & m, g));
+            out[e] = resid(up, dn, lf, rt, ldg(in + e), ldg(rhs + e));
+        }
+    }
+}
+
 template <typename T, int EPT>
 __global__ void __launch_bounds__(kBatchThreads, 4) batch_kernel(const BatchParams bp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -288,63 +375,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batch_kernel(const BatchPara
                 }
                 const cpx<T> *in = reinterpret_cast<const cpx<T> *>(S.in) + sf.off;
                 const cpx<T> *rhs = reinterpret_cast<const cpx<T> *>(S.aux) + sf.off;
-                const T inv_h2 = (T)((double)g.n * S.a * (double)g.n * S.a);
-                const int64_t m = g.n - 1;
-                auto resid = [&](const cpx<T> &up, const cpx<T> &dn, const cpx<T> &lf, const cpx<T> &rt,
-                                 const cpx<T> &c, const cpx<T> &r) -> cpx<T> {
-                    const T lx = up.x + dn.x + lf.x + rt.x - (T)4 * c.x;
-                    const T ly = up.y + dn.y + lf.y + rt.y - (T)4 * c.y;
-                    return {lx * inv_h2 - r.x, ly * inv_h2 - r.y};
-                };
-                if constexpr (sizeof(T) == 4) {
-                    // Pairs (e, e + 1), e even: the two share rank and row (L is even), so
-                    // their up / down neighbours are again two adjacent elements, and so
-                    // are left / right except at a block edge.  Adjacent 16-byte-aligned
-                    // pairs move as one 16-byte access, anything else element by element.
-                    auto ld2 = [](const cpx<T> *p0, const cpx<T> *p1, cpx<T> &v0, cpx<T> &v1) {
-                        if (p1 == p0 + 1 && ((uintptr_t)p0 & 15) == 0) {
-                            const float4 q = __ldg(reinterpret_cast<const float4 *>(p0));
-                            v0 = {q.x, q.y};
-                            v1 = {q.z, q.w};
-                        } else {
-                            v0 = ldg(p0);
-                            v1 = ldg(p1);
-                        }
-                    };
-                    for (int i = tid; i < TP / 2; i += nthr) {
-                        const int64_t e = e0 + 2 * i;
-                        const int64_t gi0 = real_gidx(e, g), gc1 = real_gidx(e + 1, g) & m;
-                        const int64_t gr = gi0 >> g.logN, gc0 = gi0 & m;
-                        const int64_t au = real_elem((gr - 1) & m, gc0, g), ad = real_elem((gr + 1) & m, gc0, g);
-                        cpx<T> up0, up1, dn0, dn1, lf0, lf1, rt0, rt1, c0, c1, r0, r1;
-                        ld2(in + au, in + au + 1, up0, up1);
-                        ld2(in + ad, in + ad + 1, dn0, dn1);
-                        ld2(in + real_elem(gr, (gc0 - 1) & m, g), in + real_elem(gr, (gc1 - 1) & m, g), lf0, lf1);
-                        ld2(in + real_elem(gr, (gc0 + 1) & m, g), in + real_elem(gr, (gc1 + 1) & m, g), rt0, rt1);
-                        ld2(in + e, in + e + 1, c0, c1);
-                        ld2(rhs + e, rhs + e + 1, r0, r1);
-                        const cpx<T> o0 = resid(up0, dn0, lf0, rt0, c0, r0);
-                        const cpx<T> o1 = resid(up1, dn1, lf1, rt1, c1, r1);
-                        cpx<T> *po = out + e;
-                        if (((uintptr_t)po & 15) == 0) {
-                            *reinterpret_cast<float4 *>(po) = make_float4(o0.x, o0.y, o1.x, o1.y);
-                        } else {
-                            po[0] = o0;
-                            po[1] = o1;
-                        }
-                    }
-                } else {
-                    for (int i = tid; i < TP; i += nthr) {
-                        const int64_t e = e0 + i;
-                        const int64_t gi = real_gidx(e, g);
-                        const int64_t gr = gi >> g.logN, gc = gi & m;
-                        const cpx<T> up = ldg(in + real_elem((gr - 1) & m, gc, g));
-                        const cpx<T> dn = ldg(in + real_elem((gr + 1) & m, gc, g));
-                        const cpx<T> lf = ldg(in + real_elem(gr, (gc - 1) & m, g));
-                        const cpx<T> rt = ldg(in + real_elem(gr, (gc + 1) & m, g));
-                        out[e] = resid(up, dn, lf, rt, ldg(in + e), ldg(rhs + e));
-                    }
-                }
+                residual_tile<T, TP>(sf.g, S.a, in, rhs, out, e0, nthr, tid);
             }
             continue;
         }
