@@ -37,6 +37,26 @@ template <> ZM_DEV cpx<float> csub(cpx<float> a, cpx<float> b) {
     memcpy(&r, &D, 8);
     return r;
 }
+// per component a * b + c (fused, one rounding) and a * b, one FP32x2 instruction each
+ZM_DEV cpx<float> cfma2(cpx<float> a, cpx<float> b, cpx<float> c) {
+    unsigned long long A, B, Cc, D;
+    memcpy(&A, &a, 8);
+    memcpy(&B, &b, 8);
+    memcpy(&Cc, &c, 8);
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(D) : "l"(A), "l"(B), "l"(Cc));
+    cpx<float> r;
+    memcpy(&r, &D, 8);
+    return r;
+}
+ZM_DEV cpx<float> cmul2(cpx<float> a, cpx<float> b) {
+    unsigned long long A, B, D;
+    memcpy(&A, &a, 8);
+    memcpy(&B, &b, 8);
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(D) : "l"(A), "l"(B));
+    cpx<float> r;
+    memcpy(&r, &D, 8);
+    return r;
+}
 
 // Twiddle storage: FP64 pair for complex128, split hi/lo FP32 pairs for complex64
 // (w = hi + lo with hi = fl32(w), lo = fl32(w - hi), both from an FP64 value).

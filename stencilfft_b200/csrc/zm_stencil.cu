@@ -703,9 +703,25 @@ __global__ void __launch_bounds__(256) stencil3d_march_kernel(const cpx<S> *__re
             ry = O::fmaop((S)(-6), cc.y, ry);
             return C{O::mul(rx, coef), O::mul(ry, coef)};
         };
-        if (PAIRS && VEC >= 2) {
+        bool paired = false;
+        if constexpr (PAIRS) {
+          if (VEC >= 2) {
+            paired = true;
             // complex64, two adjacent elements per thread (same row, same vector j): every
-            // slot access and the store are 16-byte vectors, except across a block edge
+            // slot access and the store are 16-byte vectors, except across a block edge;
+            // each element's sums run on its (re, im) pair as one FP32x2 instruction (the
+            // same operations in the same order per component as lap)
+            auto lapv = [&](const C &up, const C &dn, const C &lf, const C &rt, const C &fr, const C &bk,
+                            const C &cc) {
+                C r = cadd(C{0.f, 0.f}, up);
+                r = cadd(r, dn);
+                r = cadd(r, lf);
+                r = cadd(r, rt);
+                r = cadd(r, fr);
+                r = cadd(r, bk);
+                r = cfma2(C{-6.f, -6.f}, cc, r);
+                return cmul2(r, C{coef, coef});
+            };
             using C2 = float4;
             auto ld2 = [](const C *p, C &a, C &b) {
                 const C2 q = *reinterpret_cast<const C2 *>(p);
@@ -735,10 +751,12 @@ __global__ void __launch_bounds__(256) stencil3d_march_kernel(const cpx<S> *__re
                 ld2(pm + c, fr0, fr1);
                 ld2(pp + c, bk0, bk1);
                 ld2(pc + c, c0, c1);
-                const C o0 = lap(up0, dn0, lf0, rt0, fr0, bk0, c0), o1 = lap(up1, dn1, lf1, rt1, fr1, bk1, c1);
+                const C o0 = lapv(up0, dn0, lf0, rt0, fr0, bk0, c0), o1 = lapv(up1, dn1, lf1, rt1, fr1, bk1, c1);
                 *reinterpret_cast<C2 *>(orow + e) = make_float4((float)o0.x, (float)o0.y, (float)o1.x, (float)o1.y);
             }
-        } else {
+          }
+        }
+        if (!paired) {
             for (int e = tid; e < per_plane; e += blockDim.x) {
                 const int r = e >> logL, pos = e & (L - 1);      // tile row, packed position
                 const int c = (r + 1) * L + pos;                   // centre's slot element
