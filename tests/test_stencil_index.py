@@ -1,4 +1,5 @@
-"""CPU check of the 3D Laplacian kernel's neighbour addressing against the oracle's layout.
+"""CPU checks of the stencil kernels' neighbour addressing against the oracle's layout
+(the 3D Laplacian kernels; the batch residual step's in-block offsets at the end).
 
 ``stencil3d_lines_kernel`` (stencilfft_b200/csrc/zm_stencil.cu) finds the y / z
 neighbour lines through the block-cyclic maps and the x neighbours across a block edge
@@ -209,3 +210,34 @@ def test_laplace3d_plane_tiles_match_layout(n, b, p):
             for nm in ref:
                 assert (got[nm] >= 0).all(), (nm, ty, zsteps)
                 assert np.array_equal(got[nm], ref[nm]), (nm, ty, zsteps)
+
+
+@pytest.mark.parametrize("n,b,p", [(32, 4, 2), (64, 4, 2), (64, 8, 2), (128, 8, 4), (128, 16, 2), (256, 32, 2),
+                                   (64, 16, 2), (128, 4, 4)])
+def test_batch_residual_interior_offsets_match_layout(n, b, p):
+    """The batch residual step (zm_batch.cu, residual_tile) takes the four neighbours of an
+    element pair (e, e + 1), e even, at e -+ L (rows) and e -+ VEC (columns) when the pair
+    lies inside its rank's B x B block (in-block column j = pos >> log VEC and row lr mod B
+    both off the block's edges) and VEC >= 2.  Check every such pair against the true
+    neighbours of the 2D real layout (the oracle's restatement of utils.h), and that the
+    pair shares its in-block column."""
+    L = n // p
+    vec = L // b
+    fwd = O.real_layout_map(2, n, b, p)
+    inv = O.real_layout_inverse_map(2, n, b, p)
+    r, c = fwd // n, fwd % n
+    nat = lambda rr, cc: (rr % n) * n + cc % n
+    true = {"up": inv[nat(r - 1, c)], "dn": inv[nat(r + 1, c)], "lf": inv[nat(r, c - 1)], "rt": inv[nat(r, c + 1)]}
+    e = np.arange(0, L * L * p * p, 2, dtype=np.int64)
+    pos, lr = e & (L - 1), (e >> lg(L)) & (L - 1)
+    j, rb = pos >> lg(vec), lr & (b - 1)
+    fast = (vec >= 2) & (j > 0) & (j < b - 1) & (rb > 0) & (rb < b - 1)
+    if vec >= 2:
+        assert fast.any()
+    assert np.array_equal((pos + 1) >> lg(vec), j)          # e + 1 in the same in-block column
+    for k in (0, 1):
+        ee = e[fast] + k
+        assert np.array_equal(true["up"][ee], ee - L)
+        assert np.array_equal(true["dn"][ee], ee + L)
+        assert np.array_equal(true["lf"][ee], ee - vec)
+        assert np.array_equal(true["rt"][ee], ee + vec)
