@@ -356,24 +356,57 @@ ZM_DEV void stencil_rows_body(const S *__restrict__ in, S *__restrict__ out, S *
         const V lf2 = colv(e, lr0 + r, -2), rt2 = colv(e, lr0 + r, 2);
         const V &up = ys[r + 1], &dn = ys[r + 3], &up2 = ys[r], &dn2 = ys[r + 4], &c = ys[r + 2];
         V res, rx, ry;
+        if constexpr (sizeof(S) == 4) {
+            // FP32: the same operations in the same order on two scalars at a time, one
+            // FP32x2 instruction each
+            using F2 = cpx<float>;
+            auto pr = [](const V &v, int i) { return F2{v.v[2 * i], v.v[2 * i + 1]}; };
+            const F2 z{0.f, 0.f}, m8{-8.f, -8.f}, p8{8.f, 8.f}, m4{-4.f, -4.f}, cf{coef, coef}, rd{rden, rden};
 #pragma unroll
-        for (int i = 0; i < V::n; i++) {
-            S s = O::add((S)0, up.v[i]);
-            s = O::add(s, dn.v[i]);
-            s = O::add(s, lf.v[i]);
-            s = O::add(s, rt.v[i]);
-            s = O::fmaop((S)(-4), c.v[i], s);
-            res.v[i] = O::mul(s, coef);
-            S x = O::add((S)0, O::mul(lf.v[i], (S)-8));
-            x = O::add(x, lf2.v[i]);
-            x = O::add(x, O::mul(rt.v[i], (S)8));
-            x = O::sub(x, rt2.v[i]);
-            rx.v[i] = div_den(x, den, rden);
-            S y = O::add((S)0, O::mul(up.v[i], (S)-8));
-            y = O::add(y, up2.v[i]);
-            y = O::add(y, O::mul(dn.v[i], (S)8));
-            y = O::sub(y, dn2.v[i]);
-            ry.v[i] = div_den(y, den, rden);
+            for (int i = 0; i < V::n / 2; i++) {
+                F2 t = cadd(z, pr(up, i));
+                t = cadd(t, pr(dn, i));
+                t = cadd(t, pr(lf, i));
+                t = cadd(t, pr(rt, i));
+                t = cfma2(m4, pr(c, i), t);
+                t = cmul2(t, cf);
+                res.v[2 * i] = t.x;
+                res.v[2 * i + 1] = t.y;
+                F2 x = cadd(z, cmul2(pr(lf, i), m8));
+                x = cadd(x, pr(lf2, i));
+                x = cadd(x, cmul2(pr(rt, i), p8));
+                x = csub(x, pr(rt2, i));
+                x = cmul2(x, rd);
+                rx.v[2 * i] = x.x;
+                rx.v[2 * i + 1] = x.y;
+                F2 y = cadd(z, cmul2(pr(up, i), m8));
+                y = cadd(y, pr(up2, i));
+                y = cadd(y, cmul2(pr(dn, i), p8));
+                y = csub(y, pr(dn2, i));
+                y = cmul2(y, rd);
+                ry.v[2 * i] = y.x;
+                ry.v[2 * i + 1] = y.y;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < V::n; i++) {
+                S s = O::add((S)0, up.v[i]);
+                s = O::add(s, dn.v[i]);
+                s = O::add(s, lf.v[i]);
+                s = O::add(s, rt.v[i]);
+                s = O::fmaop((S)(-4), c.v[i], s);
+                res.v[i] = O::mul(s, coef);
+                S x = O::add((S)0, O::mul(lf.v[i], (S)-8));
+                x = O::add(x, lf2.v[i]);
+                x = O::add(x, O::mul(rt.v[i], (S)8));
+                x = O::sub(x, rt2.v[i]);
+                rx.v[i] = div_den(x, den, rden);
+                S y = O::add((S)0, O::mul(up.v[i], (S)-8));
+                y = O::add(y, up2.v[i]);
+                y = O::add(y, O::mul(dn.v[i], (S)8));
+                y = O::sub(y, dn2.v[i]);
+                ry.v[i] = div_den(y, den, rden);
+            }
         }
         *reinterpret_cast<uint4 *>(out + e * NC) = *reinterpret_cast<const uint4 *>(&res);
         *reinterpret_cast<uint4 *>(out2 + e * NC) = *reinterpret_cast<const uint4 *>(&rx);
