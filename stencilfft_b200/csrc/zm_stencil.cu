@@ -317,14 +317,30 @@ ZM_DEV void stencil_rows_body(const S *__restrict__ in, S *__restrict__ out, S *
                 // laplace.cu:91-168 accumulation order
                 const V lf = colv(e, lr0 + r, -1), rt = colv(e, lr0 + r, 1);
                 const V &up = ys[r], &dn = ys[r + 2], &c = ys[r + 1];
+                if constexpr (sizeof(S) == 4) {   // two scalars per FP32x2 instruction, same order
+                    using F2 = cpx<float>;
+                    auto pr = [](const V &v, int i) { return F2{v.v[2 * i], v.v[2 * i + 1]}; };
 #pragma unroll
-                for (int i = 0; i < V::n; i++) {
-                    S s = O::add((S)0, up.v[i]);
-                    s = O::add(s, dn.v[i]);
-                    s = O::add(s, lf.v[i]);
-                    s = O::add(s, rt.v[i]);
-                    s = O::fmaop((S)(-4), c.v[i], s);
-                    res.v[i] = O::mul(s, coef);
+                    for (int i = 0; i < V::n / 2; i++) {
+                        F2 t = cadd(F2{0.f, 0.f}, pr(up, i));
+                        t = cadd(t, pr(dn, i));
+                        t = cadd(t, pr(lf, i));
+                        t = cadd(t, pr(rt, i));
+                        t = cfma2(F2{-4.f, -4.f}, pr(c, i), t);
+                        t = cmul2(t, F2{coef, coef});
+                        res.v[2 * i] = t.x;
+                        res.v[2 * i + 1] = t.y;
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < V::n; i++) {
+                        S s = O::add((S)0, up.v[i]);
+                        s = O::add(s, dn.v[i]);
+                        s = O::add(s, lf.v[i]);
+                        s = O::add(s, rt.v[i]);
+                        s = O::fmaop((S)(-4), c.v[i], s);
+                        res.v[i] = O::mul(s, coef);
+                    }
                 }
             } else {
                 // dx.cu:26-79 / dy.cu:34-100: ((-8 f[-1] + f[-2]) + 8 f[+1]) - f[+2], / (12 delta)
@@ -335,13 +351,28 @@ ZM_DEV void stencil_rows_body(const S *__restrict__ in, S *__restrict__ out, S *
                 } else {
                     m1 = ys[r + 1]; m2 = ys[r]; p1 = ys[r + 3]; p2 = ys[r + 4];
                 }
+                if constexpr (sizeof(S) == 4) {   // two scalars per FP32x2 instruction, same order
+                    using F2 = cpx<float>;
+                    auto pr = [](const V &v, int i) { return F2{v.v[2 * i], v.v[2 * i + 1]}; };
 #pragma unroll
-                for (int i = 0; i < V::n; i++) {
-                    S s = O::add((S)0, O::mul(m1.v[i], (S)-8));
-                    s = O::add(s, m2.v[i]);
-                    s = O::add(s, O::mul(p1.v[i], (S)8));
-                    s = O::sub(s, p2.v[i]);
-                    res.v[i] = div_den(s, den, rden);
+                    for (int i = 0; i < V::n / 2; i++) {
+                        F2 t = cadd(F2{0.f, 0.f}, cmul2(pr(m1, i), F2{-8.f, -8.f}));
+                        t = cadd(t, pr(m2, i));
+                        t = cadd(t, cmul2(pr(p1, i), F2{8.f, 8.f}));
+                        t = csub(t, pr(p2, i));
+                        t = cmul2(t, F2{rden, rden});
+                        res.v[2 * i] = t.x;
+                        res.v[2 * i + 1] = t.y;
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < V::n; i++) {
+                        S s = O::add((S)0, O::mul(m1.v[i], (S)-8));
+                        s = O::add(s, m2.v[i]);
+                        s = O::add(s, O::mul(p1.v[i], (S)8));
+                        s = O::sub(s, p2.v[i]);
+                        res.v[i] = div_den(s, den, rden);
+                    }
                 }
             }
             *reinterpret_cast<uint4 *>(out + e * NC) = *reinterpret_cast<const uint4 *>(&res);
