@@ -218,20 +218,34 @@ __device__ __noinline__ void batch_tile(int op, bool scale, double a, const Batc
         // d_ct(rid L + d_lp(pos)) = d_ct(k2 M + k1) = k1 VEC + k2 = r, the slot position
         // itself; along the lines d_ct(cid L + d_lp(p)) of line l0 + t.  The factor
         // -1 / (a^2 |k|^2) in the working precision (|k|^2 an exact integer).
-        const int tot = sf.T << g.logN;
-        const int nh = (int)(g.n >> 1);
         const T a2 = (T)(a * a);
-        for (int e = tid; e < tot; e += nthr) {
-            const int t = e >> g.logN, r = e & (int)(g.n - 1);
-            const int64_t l = l0 + t, cid = l >> g.logL, p = l & (g.L - 1);
-            const int ka = (int)d_ct(cid * g.L + d_lp(p, g), g);
-            const int sa = ka >= nh ? ka - (int)g.n : ka, sb = r >= nh ? r - (int)g.n : r;
+        auto divide = [&](int e, int ka, int r, int nh, int n) {
+            const int sa = ka >= nh ? ka - n : ka, sb = r >= nh ? r - n : r;
             const int ksq = sa * sa + sb * sb;
             T fac;
             if constexpr (sizeof(T) == 4) fac = ksq == 0 ? 0.f : -__frcp_rn(a2 * (float)ksq);
             else fac = ksq == 0 ? 0.0 : -1.0 / (a2 * (double)ksq);
             const cpx<T> v = s[SW::f(e)];
             s[SW::f(e)] = {v.x * fac, v.y * fac};
+        };
+        if constexpr (LMC > 0) {
+            // the same with the sizes fixed: ka = ct(cid L + lp(p)) in 32-bit constant shifts
+            using G = V4Geom<LMC, LP, false>;
+            constexpr int M = 1 << LMC, LVP = G::LVP, VP = G::VP;
+#pragma unroll 4
+            for (int e = tid; e < EPT * kBatchThreads; e += kBatchThreads) {
+                const int t = e >> G::LN, r = e & (G::N - 1);
+                const int l = (int)l0 + t, cid = l >> G::LL, p = l & (G::L - 1);
+                const int q = (cid << G::LL) + (p >> LVP) + ((p & (VP - 1)) << LMC);
+                divide(e, ((q & (M - 1)) << 2) + (q >> LMC), r, G::N / 2, G::N);
+            }
+        } else {
+            const int tot = sf.T << g.logN;
+            for (int e = tid; e < tot; e += nthr) {
+                const int t = e >> g.logN, r = e & (int)(g.n - 1);
+                const int64_t l = l0 + t, cid = l >> g.logL, p = l & (g.L - 1);
+                divide(e, (int)d_ct(cid * g.L + d_lp(p, g), g), r, (int)(g.n >> 1), (int)g.n);
+            }
         }
         __syncthreads();
         batch_tile_transform<T, EPT, true, LMC, SW>(s, sf, nthr, tid, twN);
