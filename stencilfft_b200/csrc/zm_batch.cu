@@ -289,12 +289,13 @@ __device__ __noinline__ void residual_tile(const Geom &g, double a, const cpx<T>
         // block cycle), adjacent pairs again when VEC >= 2.
         const bool fast = g.logVEC >= 1 &&
                           (((uintptr_t)in | (uintptr_t)rhs | (uintptr_t)out) & 15) == 0;
-        const int iL = (int)g.L, iV = (int)g.vec, bm = (int)g.b - 1;
+        // the geometry in registers (g lives in shared memory; a field holds < 2^31 elements)
+        const int iL = (int)g.L, iV = (int)g.vec, bm = (int)g.b - 1, logL = g.logL, logV = g.logVEC;
         auto q4 = [](const cpx<T> *q) { return __ldg(reinterpret_cast<const float4 *>(q)); };
         for (int i = tid; i < TP / 2; i += nthr) {
             const int64_t e = e0 + 2 * i;
-            const int pos = (int)(e & (g.L - 1)), lr = (int)((e >> g.logL) & (g.L - 1));
-            const int j = pos >> g.logVEC, rb = lr & bm;
+            const int pos = (int)e & (iL - 1), lr = ((int)e >> logL) & (iL - 1);
+            const int j = pos >> logV, rb = lr & bm;
             if (fast && j > 0 && j < bm && rb > 0 && rb < bm) {
                 const cpx<T> *pc = in + e;
                 const float4 up = q4(pc - iL), dn = q4(pc + iL), lf = q4(pc - iV), rt = q4(pc + iV);
